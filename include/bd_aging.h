@@ -1,0 +1,191 @@
+/*
+ * bd_aging.h -- C ABI of the B200 Brownian-dynamics engine (libbd_aging_b200.so).
+ *
+ * Two layers:
+ *
+ *  1. Reference-mirror entry points.  One function per entry point of the
+ *     reference (encabezados.h:86-158), same argument meaning, operating on
+ *     device-accessible pointers (cudaMalloc'd or managed memory) with the
+ *     reference's float3 array-of-structs layout (3 floats per particle).
+ *     Differences: every call returns an int status (BD_OK or a BD_ERR_*
+ *     code) instead of calling exit(), takes an explicit CUDA stream
+ *     (NULL = legacy default stream), and never writes out of bounds.
+ *
+ *  2. The batched replica engine (bd_engine_*): many independent systems of
+ *     uneven size stepped together by fused sm_100a kernels.  Positions enter
+ *     and leave through host float3 arrays in the reference's particle order
+ *     (big particles first, main.cu:377-394).
+ *
+ * All functions are thread-compatible (no hidden global state apart from
+ * per-device kernel attributes); handles are not shared across threads.
+ */
+#ifndef BD_AGING_H
+#define BD_AGING_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BD_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+#define BD_OK                 0
+#define BD_ERR_ARG            1   /* invalid argument (NULL, size, species char) */
+#define BD_ERR_CUDA           2   /* a CUDA runtime call failed                  */
+#define BD_ERR_CELL_OVERFLOW  3   /* a cell held more particles than its capacity
+                                     (reference: "ntags reached limit", exit 1,
+                                     main.cu:655-659)                            */
+#define BD_ERR_NOMEM          4
+#define BD_ERR_STATE          5   /* call out of order (e.g. run before load)    */
+#define BD_ERR_TIMEOUT        6   /* a bounded device wait expired               */
+#define BD_ERR_FILE           7   /* file missing / unreadable (reference exit -2)*/
+#define BD_ERR_FORMAT         8   /* malformed input (reference exit 1)          */
+#define BD_ERR_NUMERIC        9   /* non-finite position detected                */
+
+const char *bd_status_string(int status);
+int bd_abi_version(void);
+
+/* ---- parameter block: layout-identical to the reference `parametros`
+ *      (encabezados.h:40-75) so a reference caller can pass its own struct. */
+typedef struct bd_parametros {
+    float side;
+    float dt;
+    float mass_big;
+    float mass_sml;
+    float sigma_big;
+    float sigma_sml;
+    float cell_side_big;
+    float cell_side_sml;
+    float temp_set;
+    float bin_size_dplt;
+    float bin_size_gder;
+    float range_dplt;
+    float range_gder;
+    int ngrain_big;
+    int ngrain_sml;
+    int ngrain_tot;
+    int ntags_big;
+    int ntags_sml;
+    int ncell_big;
+    int ncell_med;
+    int ncell_sml;
+    int nrange_bb;
+    int nrange_bs;
+    int nrange_sb;
+    int nrange_ss;
+    int nbins_dplt;
+    int nbins_gder;
+    int nsearch_big;
+    int not_finished;
+    int NH;
+    int WCA_flag;
+    long idum;
+} bd_parametros;
+
+/* Parameter set-up of the reference driver (main.cu:155-163, 244-298,
+ * 348-349): cell counts (int)(side/(1.05 sigma)), cell sides, neighbour
+ * ranges nrange_bb/bs/sb/ss, gder bin size.  Host-only. */
+int bd_setup_params(bd_parametros *pars, float side, int ngrain_big, int ngrain_sml, float sigma_big,
+                    float sigma_sml, float mass_big, float mass_sml, int ntags_big, int ntags_sml,
+                    int nbins_gder, float range_gder, double dt, float temp0);
+
+/* ---- reference-mirror entry points (device pointers) -------------------- */
+
+/* cell_locate_dev (cell_locate.cu:155-209) together with the clears that the
+ * reference launches before it (set_vec_int_dev, main.cu:536-541).  type is
+ * 'b' or 's'.  Output: nocup[ncell^3] occupancies and cell_vec[ncell^3 *
+ * ntags] particle indices, occupied slots in ascending particle order (the
+ * order of cell_locate_hst; the reference device order is arbitrary), unused
+ * slots -1.  A cell above ntags particles returns BD_ERR_CELL_OVERFLOW and
+ * writes only the first ntags slots. */
+int bd_cell_locate(char type, const float *rr, int *nocup, int *cell_vec, const bd_parametros *pars,
+                   void *stream);
+
+/* get_forces_same_dev (get_forces.cu:297-424): WCA-modified forces, potential
+ * and virial between particles of species `type`, ADDED to ff/vir/pot like
+ * the reference (callers clear them first, main.cu:556-561).  nocup/cell_vec
+ * come from bd_cell_locate for the same species. */
+int bd_get_forces_same(char type, const float *rr, float *ff, float *vir, float *pot, const int *nocup,
+                       const int *cell_vec, const bd_parametros *pars, void *stream);
+
+/* get_forces_diff_dev (get_forces.cu:428-558): forces on `type` particles
+ * from `type_other` particles, using the other species' cell list. */
+int bd_get_forces_diff(char type, char type_other, const float *rr, float *ff, const float *rr_other,
+                       float *vir, float *pot, const int *nocup_other, const int *cell_other,
+                       const bd_parametros *pars, void *stream);
+
+/* Size in bytes of the per-particle generator state used by bd_setup_rng /
+ * bd_update_ermak (the reference's curandState, update_ermak.cu:83-89). */
+size_t bd_rng_state_size(void);
+
+/* setup_rng_kernel (update_ermak.cu:85-89): curand_init(seed, idx, 0) for
+ * idx < n.  The reference seeds big with idum and small with idum+1
+ * (main.cu:483-484). */
+int bd_setup_rng(void *states, unsigned long long seed, int n, void *stream);
+
+/* update_ermak_dev (update_ermak.cu:91-160): Ermak-McCammon step with the
+ * reference's cuRAND XORWOW stream: r += F dt/sigma + sqrt(2 T dt/sigma) xi,
+ * periodic wrap of rr, rr_raw advanced without wrap.  T = pars->temp_set. */
+int bd_update_ermak(char type, float *rr, float *rr_raw, const float *ff, void *states,
+                    const bd_parametros *pars, void *stream);
+
+/* Same update with caller-supplied N(0,1) values noise[3*i+{0,1,2}]
+ * (parity tests inject identical noise into the reference's host twin,
+ * update_ermak.cu:8-77). */
+int bd_update_ermak_noise(char type, float *rr, float *rr_raw, const float *ff, const float *noise,
+                          const bd_parametros *pars, void *stream);
+
+/* calculate_temp_linear / calculate_temp_sine (set_temp.cu:7-23), same
+ * float arithmetic, including the reference's NaN at t == t0 == tf. */
+float bd_calculate_temp_linear(float T0, float Tf, float t0, float tf, float t);
+float bd_calculate_temp_sine(float T0, float Tf, float t0, float tf, float period, float t);
+
+/* get_gder_dev (get_gder.cu:69-127) for one species pair: ordered pairs with
+ * minimum-image distance < range_gder binned by (int)(dist/bin_size), with the
+ * reference's float operation order.  Counts are ADDED to the caller's
+ * device array counts[nbins_gder] as exact 64-bit integers (the reference
+ * accumulates floats per block, exact below 2^24 per bin). */
+int bd_get_gder(char type, char type_other, const float *rr, const float *rr_other,
+                unsigned long long *counts, const bd_parametros *pars, void *stream);
+
+/* g(r) normalisation of main.cu:849-877 for one sample, host arithmetic
+ * identical to the reference: counts[4][nbins] (bb, bs, sb, ss) summed over
+ * configs -> gder[4][nbins] averaged over n_configs.  Host pointers. */
+int bd_gder_normalize(const double *counts, int nbins, float bin_size, float side, int ngrain_big,
+                      int ngrain_sml, float sigma_big, float sigma_sml, int n_configs, float *gder);
+
+/* fself_isotropic (fself.cu:3-21): adds (1/N) sum sin(q|dr|)/(q|dr|) over
+ * dr = rr_raw - rr0 to fself_host[sample_number].  Device inputs, host
+ * output, stream-synchronous. */
+int bd_fself_isotropic(const float *rr_raw, const float *rr0, int ngrain, float *fself_host, int sample_number,
+                       float qmax, void *stream);
+
+/* Mean squared displacement of main.cu:776-792 for one species: returns
+ * (1/N) sum |rr_raw - rr0|^2 in *msd_host.  Stream-synchronous. */
+int bd_msd(const float *rr_raw, const float *rr0, int ngrain, float *msd_host, void *stream);
+
+/* ---- Contracting_Vector3D (Contracting_Vector3D.cuh:39-75) --------------- */
+typedef struct bd_cv3d bd_cv3d;
+/* constructor (Contracting_Vector3D.cu:11-55) */
+int bd_cv3d_create(int bins, float range, bd_cv3d **out);
+/* add_statistics (Contracting_Vector3D.cu:57-164): device rr/xx float3 arrays;
+ * side <= 0 means no periodic images (std::nullopt in the reference).  The
+ * normal equations are accumulated on the GPU in FP64. */
+int bd_cv3d_add_statistics(bd_cv3d *cv, const float *rr, const float *xx, int nparticles, float side,
+                           void *stream);
+/* calculate_vector (Contracting_Vector3D.cu:166-297): SVD pseudo-inverse
+ * solve per Cartesian component, averaged over the three.  Returns
+ * BD_ERR_STATE when no statistics were added (the reference throws). */
+int bd_cv3d_calculate_vector(bd_cv3d *cv);
+/* get_vector (Contracting_Vector3D.cu:299-304); BD_ERR_STATE before
+ * calculate_vector (the reference throws). Host output of `bins` floats. */
+int bd_cv3d_get_vector(const bd_cv3d *cv, float *out);
+int bd_cv3d_destroy(bd_cv3d *cv);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BD_AGING_H */

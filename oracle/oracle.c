@@ -1,0 +1,513 @@
+/*
+ * oracle.c -- CPU restatement of the reference hot path.  TEST INFRASTRUCTURE:
+ * only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline/reference
+ * legs load it, always as the checker.  Compiled with -ffp-contract=off so
+ * that every a*b+c rounds twice, as in the reference's host functions.
+ *
+ * Each or_ref_* function states which reference lines it follows and keeps
+ * the reference's mix of float and double operations; the or_eng_* functions
+ * restate the B200 engine's own arithmetic.
+ */
+#include "oracle.h"
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define OR_PI 3.14159266f   /* encabezados.h:25 (sic) */
+#define OR_EPS 1.0f         /* encabezados.h:30 */
+
+/* ------------------------------------------------------------------ params */
+/* main.cu:155-163 (dt, temp, gder), 244-298 (cells, ranges), 348-349 (NH). */
+void or_ref_setup_params(bd_parametros *p, float side, int nb, int ns, float sigma_big, float sigma_sml,
+                         float mass_big, float mass_sml, int ntags_big, int ntags_sml, int nbins_gder,
+                         float range_gder, double dt, float temp0) {
+    memset(p, 0, sizeof(*p));
+    p->dt = (float)dt;
+    p->temp_set = temp0;
+    p->nbins_gder = nbins_gder;
+    p->range_gder = range_gder;
+    p->ntags_big = ntags_big;
+    p->ntags_sml = ntags_sml;
+    p->bin_size_gder = range_gder / ((float)nbins_gder);
+    p->side = side;
+    p->ngrain_big = nb;
+    p->ngrain_sml = ns;
+    p->ngrain_tot = nb + ns;
+    p->sigma_big = sigma_big;
+    p->sigma_sml = sigma_sml;
+    p->mass_big = mass_big;
+    p->mass_sml = mass_sml;
+    float cutoff = sigma_big;
+    int ncb = (int)(side / (1.05 * cutoff));
+    p->ncell_big = ncb;
+    p->cell_side_big = side / ((float)ncb);
+    cutoff = sigma_sml;
+    int ncs = (int)(side / (1.05 * cutoff));
+    p->ncell_sml = ncs;
+    p->cell_side_sml = side / ((float)ncs);
+    p->nrange_bb = 1;
+    float aux = (float)((sigma_big + sigma_sml) / 2.0);
+    p->nrange_bs = 1 + (int)(aux / p->cell_side_sml);
+    p->nrange_sb = 1;
+    p->nrange_ss = 1;
+    p->NH = 256;
+}
+
+/* --------------------------------------------------------------- cell list */
+/* cell_locate_hst, cell_locate.cu:46-104: inverse cell side computed as a
+ * double division narrowed to float; (int) truncation; ==ncell clamp;
+ * slots filled in ascending particle order.  Returns 1 when a cell reaches
+ * ntags particles (the reference's overflow condition, cell_locate.cu:91-95
+ * and main.cu:655), writing no slot beyond ntags. */
+int or_ref_cell_locate(char type, const float *rr, int *nocup, int *cell_vec, const bd_parametros *p) {
+    float csi;
+    int n, ntags, ncell;
+    if (type == 'b') { csi = (float)(1.0 / p->cell_side_big); n = p->ngrain_big; ntags = p->ntags_big; ncell = p->ncell_big; }
+    else { csi = (float)(1.0 / p->cell_side_sml); n = p->ngrain_sml; ntags = p->ntags_sml; ncell = p->ncell_sml; }
+    int nc3 = ncell * ncell * ncell, bad = 0;
+    for (int c = 0; c < nc3; c++) nocup[c] = 0;
+    for (long s = 0; s < (long)nc3 * ntags; s++) cell_vec[s] = -1;
+    for (int m = 0; m < n; m++) {
+        int ii = (int)(csi * rr[3 * m]), jj = (int)(csi * rr[3 * m + 1]), kk = (int)(csi * rr[3 * m + 2]);
+        if (ii == ncell) ii--;
+        if (jj == ncell) jj--;
+        if (kk == ncell) kk--;
+        int c = ii + ncell * (jj + ncell * kk);
+        int shift = nocup[c]++;
+        if (shift < ntags) cell_vec[c * ntags + shift] = m;
+        if (shift + 1 >= ntags) bad = 1;
+    }
+    return bad;
+}
+
+/* ------------------------------------------------------------------ forces */
+/* potential_wca_modified_hst, potentials.cu:66-76 */
+static void wca_modified(float sigma, float dist_inv, float *potential, float *normal_force) {
+    float sor = dist_inv * sigma;
+    float sor6 = sor * sor * sor;
+    sor6 = sor6 * sor6;
+    float sor12 = sor6 * sor6;
+    *potential += OR_EPS * (sor12 - 2 * sor6 + 1);
+    *normal_force = -OR_EPS * 12 * (sor12 - sor6) * dist_inv;
+}
+
+/* Shared body of get_forces_same_hst (get_forces.cu:21-145) and
+ * get_forces_diff_hst (get_forces.cu:149-277): one particle m against the
+ * cells of the other set within +-nrange, float arithmetic. */
+static void forces_sweep(const float *rrm_p, int m, int same, const float *rr_other, const int *nocup,
+                         const int *cell_vec, int ncell, int ntags, int nrange, float csi, float sigma,
+                         float side, float *ffm, float *virial, float *potential) {
+    float cutoff = 1.0f * sigma, cutoff2 = cutoff * cutoff, side_inv = 1.0f / side;
+    float rx = rrm_p[0], ry = rrm_p[1], rz = rrm_p[2];
+    int ii = (int)(csi * rx), jj = (int)(csi * ry), kk = (int)(csi * rz);
+    if (ii == ncell) ii--;
+    if (jj == ncell) jj--;
+    if (kk == ncell) kk--;
+    for (int di = -nrange; di <= nrange; di++)
+        for (int dj = -nrange; dj <= nrange; dj++)
+            for (int dk = -nrange; dk <= nrange; dk++) {
+                int iip = (ii + di + ncell) % ncell, jjp = (jj + dj + ncell) % ncell, kkp = (kk + dk + ncell) % ncell;
+                int c = iip + ncell * (jjp + ncell * kkp);
+                int occ = nocup[c];
+                for (int t = 0; t < occ; t++) {
+                    int nn = cell_vec[c * ntags + t];
+                    if (same && nn == m) continue;
+                    float dx = rr_other[3 * nn] - rx, dy = rr_other[3 * nn + 1] - ry, dz = rr_other[3 * nn + 2] - rz;
+                    dx -= side * floorf(side_inv * dx + 0.5f);
+                    dy -= side * floorf(side_inv * dy + 0.5f);
+                    dz -= side * floorf(side_inv * dz + 0.5f);
+                    float dist2 = dx * dx + dy * dy + dz * dz;
+                    if (dist2 < cutoff2) {
+                        float dist_inv = sqrtf(1.0f / dist2), nf;
+                        wca_modified(sigma, dist_inv, potential, &nf);
+                        float fx = nf * dist_inv * dx, fy = nf * dist_inv * dy, fz = nf * dist_inv * dz;
+                        ffm[0] += fx; ffm[1] += fy; ffm[2] += fz;
+                        *virial -= 0.5f * (dx * fx + dy * fy + dz * fz);
+                    }
+                }
+            }
+}
+
+void or_ref_forces_same(char type, const float *rr, float *ff, float *vir, float *pot, const int *nocup,
+                        const int *cell_vec, const bd_parametros *p) {
+    int b = (type == 'b');
+    float sigma = b ? p->sigma_big : p->sigma_sml;
+    int n = b ? p->ngrain_big : p->ngrain_sml;
+    float csi = 1.0f / (b ? p->cell_side_big : p->cell_side_sml);
+    int ntags = b ? p->ntags_big : p->ntags_sml, ncell = b ? p->ncell_big : p->ncell_sml;
+    int nrange = b ? p->nrange_bb : p->nrange_ss;
+    for (int m = 0; m < n; m++)
+        forces_sweep(rr + 3 * m, m, 1, rr, nocup, cell_vec, ncell, ntags, nrange, csi, sigma, p->side, ff + 3 * m,
+                     vir + m, pot + m);
+}
+
+void or_ref_forces_diff(char type, char type_other, const float *rr, float *ff, const float *rr_other,
+                        float *vir, float *pot, const int *nocup_o, const int *cell_o, const bd_parametros *p) {
+    (void)type_other;
+    int b = (type == 'b');
+    int n = b ? p->ngrain_big : p->ngrain_sml;
+    float csi = 1.0f / (b ? p->cell_side_sml : p->cell_side_big);
+    float sigma = b ? 0.5f * (p->sigma_big + p->sigma_sml) : 0.5f * (p->sigma_sml + p->sigma_big);
+    int ntags = b ? p->ntags_sml : p->ntags_big, ncell = b ? p->ncell_sml : p->ncell_big;
+    int nrange = b ? p->nrange_bs : p->nrange_sb;
+    for (int m = 0; m < n; m++)
+        forces_sweep(rr + 3 * m, m, 0, rr_other, nocup_o, cell_o, ncell, ntags, nrange, csi, sigma, p->side,
+                     ff + 3 * m, vir + m, pot + m);
+}
+
+/* ------------------------------------------------------------------ update */
+/* update_ermak_hst, update_ermak.cu:8-77 with noise[3m+k] in place of the
+ * three gsl_ran_gaussian draws.  amplitude in double, narrowed to float. */
+void or_ref_update_ermak(char type, float *rr, float *rr_raw, const float *ff, const float *noise,
+                         const bd_parametros *p) {
+    float side = p->side, side_inv = 1.0f / side, temperature = p->temp_set, dt = p->dt;
+    int n = (type == 'b') ? p->ngrain_big : p->ngrain_sml;
+    float diameter = (type == 'b') ? p->sigma_big : p->sigma_sml;
+    float dinv = 1.0f / diameter;
+    float amplitude = (float)sqrt(2.0 * temperature * dinv * dt);
+    for (int m = 0; m < n; m++) {
+        for (int k = 0; k < 3; k++) {
+            float rnd = (float)(amplitude * (double)noise[3 * m + k]);
+            float tot = ff[3 * m + k] * dinv * dt + rnd;
+            float r = rr[3 * m + k] + tot;
+            rr_raw[3 * m + k] = rr_raw[3 * m + k] + tot;
+            r -= side * floorf(side_inv * r);
+            rr[3 * m + k] = r;
+        }
+    }
+}
+
+/* -------------------------------------------------------------------- g(r) */
+/* get_gder_hst, get_gder.cu:7-63: ordered pairs (skipping m==n for the same
+ * species), side_inv = (float)(1.0/side), floorf(side_inv*d + 0.5) with the
+ * 0.5 added in double, float sqrt, bin = (int)(dist/bin_size), ==nbins clamp.
+ * counts[nbins] are exact integers (the reference adds 1.0f per pair). */
+void or_ref_gder_counts(char type, char type_other, const float *rr, const float *rr_other, uint64_t *counts,
+                        const bd_parametros *p) {
+    int n = (type == 'b') ? p->ngrain_big : p->ngrain_sml;
+    int no = (type_other == 'b') ? p->ngrain_big : p->ngrain_sml;
+    float side = p->side, range = p->range_gder;
+    int nbins = p->nbins_gder;
+    float side_inv = (float)(1.0 / side);
+    float bin_size = range / ((float)nbins);
+    for (int m = 0; m < n; m++)
+        for (int j = 0; j < no; j++) {
+            if (type == type_other && m == j) continue;
+            float dx = rr[3 * m] - rr_other[3 * j], dy = rr[3 * m + 1] - rr_other[3 * j + 1],
+                  dz = rr[3 * m + 2] - rr_other[3 * j + 2];
+            dx -= side * floorf((float)((double)(side_inv * dx) + 0.5));
+            dy -= side * floorf((float)((double)(side_inv * dy) + 0.5));
+            dz -= side * floorf((float)((double)(side_inv * dz) + 0.5));
+            float dist = sqrtf(dx * dx + dy * dy + dz * dz);
+            if (dist < range) {
+                int bin = (int)(dist / bin_size);
+                if (bin == nbins) bin--;
+                counts[bin]++;
+            }
+        }
+}
+
+/* main.cu:847-877: shell volume 4 PI dr^3 (1/3 + n^2 + n) in double narrowed
+ * to float, free volume V - 4/3 PI sigma^3, pair densities, then / n_configs.
+ * counts: [4][nbins] totals over configs; gder out [4][nbins]. */
+void or_ref_gder_normalize(const double *counts, int nbins, float bin_size, float side, int nb, int ns,
+                           float sigma_big, float sigma_sml, int n_configs, float *gder) {
+    float volume = side * side * side;
+    float xb = (float)nb, xs = (float)ns;
+    for (int k = 0; k < nbins; k++) {
+        float xnb = (float)k;
+        float shell_vol = (float)(4.0 * OR_PI * bin_size * bin_size * bin_size * ((1.0 / 3.0) + xnb * xnb + xnb));
+        float g[4];
+        for (int j = 0; j < 4; j++) g[j] = (float)counts[j * nbins + k];
+        float sigma = sigma_big;
+        float vol_free = (float)(volume - (4.0 / 3.0) * OR_PI * sigma * sigma * sigma);
+        g[0] = g[0] / shell_vol;
+        g[0] = (float)(g[0] / (xb * (xb - 1.0) / vol_free));
+        sigma = (float)(0.5 * (sigma_big + sigma_sml));
+        vol_free = (float)(volume - (4.0 / 3.0) * OR_PI * sigma * sigma * sigma);
+        g[1] = g[1] / shell_vol;
+        g[2] = g[2] / shell_vol;
+        g[1] /= (xb * xs / vol_free);
+        g[2] /= (xs * xb / vol_free);
+        sigma = sigma_sml;
+        vol_free = (float)(volume - (4.0 / 3.0) * OR_PI * sigma * sigma * sigma);
+        g[3] = g[3] / shell_vol;
+        g[3] = (float)(g[3] / (xs * (xs - 1.0) / vol_free));
+        for (int j = 0; j < 4; j++) gder[j * nbins + k] = g[j] / n_configs;
+    }
+}
+
+/* ------------------------------------------------------------ observables */
+/* fself_isotropic, fself.cu:3-21 (float sum, sinf). */
+void or_ref_fself(const float *rr_raw, const float *rr0, int n, float *fself, int sample_number, float qmax) {
+    float sum = 0.0f;
+    for (int i = 0; i < n; i++) {
+        float dx = rr_raw[3 * i] - rr0[3 * i], dy = rr_raw[3 * i + 1] - rr0[3 * i + 1], dz = rr_raw[3 * i + 2] - rr0[3 * i + 2];
+        float mag = sqrtf(dx * dx + dy * dy + dz * dz);
+        sum += sinf(qmax * mag) / (qmax * mag);
+    }
+    sum /= n;
+    fself[sample_number] += sum;
+}
+/* main.cu:776-792 */
+float or_ref_msd(const float *rr_raw, const float *rr0, int n) {
+    float msd = 0.0f;
+    for (int i = 0; i < n; i++) {
+        float dx = rr_raw[3 * i] - rr0[3 * i], dy = rr_raw[3 * i + 1] - rr0[3 * i + 1], dz = rr_raw[3 * i + 2] - rr0[3 * i + 2];
+        msd += dx * dx + dy * dy + dz * dz;
+    }
+    return msd / (float)n;
+}
+/* main.cu:627-631: float accumulator, 0.5*pot added in double each time. */
+float or_ref_energy(const float *pot, int n) {
+    float e = 0.0f;
+    for (int i = 0; i < n; i++) e = (float)(e + 0.5 * pot[i]);
+    return e / (float)n;
+}
+/* main.cu:801-804 */
+float or_ref_pressure_z(const float *vir_b, int nb, const float *vir_s, int ns, float temp) {
+    float virial = 0.0f;
+    for (int i = 0; i < nb; i++) virial += vir_b[i];
+    for (int i = 0; i < ns; i++) virial += vir_s[i];
+    float xt = (float)(nb + ns);
+    return (float)(1.0 + virial / (3.0 * xt * temp));
+}
+
+/* ------------------------------------------------------------- schedules */
+/* set_temp.cu:7-12 */
+float or_ref_temp_linear(float T0, float Tf, float t0, float tf, float t) {
+    if (t < t0) return T0;
+    if (t > tf) return Tf;
+    float m = (Tf - T0) / (tf - t0);
+    return T0 + m * (t - t0);
+}
+/* set_temp.cu:14-23 */
+float or_ref_temp_sine(float T0, float Tf, float t0, float tf, float period, float t) {
+    if (t < t0) return T0;
+    if (t > tf) return Tf;
+    float a = (float)(0.5 * (T0 + Tf));
+    float b = (float)(0.5 * (Tf - T0));
+    float argument = (float)(2 * OR_PI * (t / period - 0.25));
+    return a + b * sinf(argument);
+}
+/* main.cu:520: time = dt * (1.0 + (float) ni), double product narrowed. */
+float or_ref_time_of_step(double dt, int ni) { return (float)(dt * (1.0 + (float)ni)); }
+
+/* log_sampling / sampling_indexes, main.cu:14-53 (float arguments). */
+int or_ref_sampling_indexes(float minimal_decade, float run_time, float dt, int per_decade, int *out, int cap) {
+    int last_power = (int)roundf(log10f(run_time));
+    int initial_power = (int)roundf(log10f(minimal_decade));
+    int decades = last_power - initial_power;
+    float values[1024];
+    float r = powf(10.0f, 1.0f / per_decade), x = 1.0f;
+    for (int i = 0; i <= per_decade && i < 1024; i++) { values[i] = x; x *= r; }
+    int total = decades * per_decade;
+    int cnt = 0;
+    if (cap > 0) out[0] = 0;
+    for (int ipow = initial_power; ipow < last_power; ++ipow) {
+        float power = (float)pow(10.0, (double)ipow);
+        for (int j = 0; j < per_decade; ++j) {
+            float scaled = values[j] * power;
+            int index = (int)roundf(scaled / dt);
+            cnt++;
+            if (cnt < cap) out[cnt] = index;
+        }
+    }
+    (void)total;
+    return cnt + 1;
+}
+
+/* rannew64.cu:55-126: subtractive lagged Fibonacci (250, 103) minus a 64-bit
+ * LCG, both mod 2^64, seeded by 1000+250 steps of a second LCG. */
+void or_rannew64_seed(or_rannew64_state *s, long idum) {
+    if (idum < 0) idum = -idum;
+    uint64_t udum = (uint64_t)idum;
+    const uint64_t uaa = 6364136223846793005ULL, ucc = 1442695040888963407ULL;
+    for (int i = 0; i < 1000; i++) udum = udum * uaa + ucc;
+    for (int i = 0; i < 250; i++) { udum = udum * uaa + ucc; s->useed[i] = udum; }
+    s->uuy = udum;
+    s->np = 249; s->nq = 102; s->init = 1;
+}
+double or_rannew64_next(or_rannew64_state *s) {
+    const uint64_t ua = 2862933555777941757ULL, uc = 3037000493ULL;
+    uint64_t uux = s->useed[s->np] - s->useed[s->nq];
+    s->useed[s->np] = uux;
+    s->np--; s->nq--;
+    if (s->np < 0) s->np = 249;
+    if (s->nq < 0) s->nq = 249;
+    s->uuy = ua * s->uuy + uc;
+    uint64_t uu = uux - s->uuy;
+    double omm = 1. / 18446744073709551615.;
+    return omm * ((double)uu);
+}
+
+/* Contracting_Vector3D::add_statistics, Contracting_Vector3D.cu:57-164, float
+ * arithmetic; the periodic image uses floor() of the double sum
+ * side_inv*d + 0.5 (Contracting_Vector3D.cu:101-105). */
+int or_ref_cv3d_add(int bins, float range, const float *rr, const float *xx, int n, float side, float *ata,
+                    float *atb) {
+    float bin_size = range / (float)bins;
+    float bin_size_inv = 1.0f / ((float)bin_size);
+    float range_square = range * range;
+    float side_inv = side > 0 ? 1.0f / side : 0.0f;
+    float *hit = (float *)calloc((size_t)bins * 3, sizeof(float));
+    int bad = 0;
+    for (int m = 0; m < n; m++) {
+        int neighs = 0;
+        for (int j = 0; j < n; j++) {
+            if (j == m) continue;
+            float dx = rr[3 * m] - rr[3 * j], dy = rr[3 * m + 1] - rr[3 * j + 1], dz = rr[3 * m + 2] - rr[3 * j + 2];
+            if (side > 0) {
+                dx -= side * (float)floor(side_inv * dx + 0.5);
+                dy -= side * (float)floor(side_inv * dy + 0.5);
+                dz -= side * (float)floor(side_inv * dz + 0.5);
+            }
+            float dist2 = dx * dx + dy * dy + dz * dz;
+            if (dist2 < range_square) {
+                float dist = sqrtf(dist2);
+                int nb = (int)(bin_size_inv * dist);
+                if (nb >= bins) nb = bins - 1; /* reference writes hit_vec[bins] here (out of bounds) */
+                hit[3 * nb] += dx / dist;
+                hit[3 * nb + 1] += dy / dist;
+                hit[3 * nb + 2] += dz / dist;
+                neighs++;
+                if (neighs == 10000) bad = 1;
+            }
+        }
+        if (neighs > 0) {
+            for (int c = 0; c < 3; c++)
+                for (int i = 0; i < bins; i++)
+                    for (int j = 0; j <= i; j++) {
+                        float aux = hit[3 * i + c] * hit[3 * j + c];
+                        ata[(size_t)c * bins * bins + (size_t)i * bins + j] += aux;
+                        if (i != j) ata[(size_t)c * bins * bins + (size_t)j * bins + i] += aux;
+                    }
+            for (int i = 0; i < bins; i++)
+                for (int c = 0; c < 3; c++) atb[c * bins + i] += hit[3 * i + c] * xx[3 * m + c];
+            memset(hit, 0, (size_t)bins * 3 * sizeof(float));
+        }
+    }
+    free(hit);
+    return bad;
+}
+
+/* ================================================================ engine */
+void or_philox4x32_10(const uint32_t ctr_in[4], const uint32_t key_in[2], uint32_t out[4]) {
+    uint32_t c0 = ctr_in[0], c1 = ctr_in[1], c2 = ctr_in[2], c3 = ctr_in[3];
+    uint32_t k0 = key_in[0], k1 = key_in[1];
+    for (int r = 0; r < 10; r++) {
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0, hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t n0 = hi1 ^ c1 ^ k0, n1 = lo1, n2 = hi0 ^ c3 ^ k1, n3 = lo0;
+        c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+        k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+void or_eng_uniform_bits(uint64_t seed, uint32_t id, uint64_t step, uint32_t stream, uint32_t out[4]) {
+    uint32_t ctr[4] = {id, (uint32_t)step, (uint32_t)(step >> 32), stream};
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    or_philox4x32_10(ctr, key, out);
+}
+/* uniform in (0,1): (x >> 8) * 2^-24 + 2^-25 (exact in float) */
+static double u01(uint32_t x) { return (double)(x >> 8) * (1.0 / 16777216.0) + (1.0 / 33554432.0); }
+void or_eng_gauss3(uint64_t seed, uint32_t id, uint64_t step, uint32_t stream, double out[3]) {
+    uint32_t b[4];
+    or_eng_uniform_bits(seed, id, step, stream, b);
+    double r0 = sqrt(-2.0 * log(u01(b[0]))), r1 = sqrt(-2.0 * log(u01(b[2])));
+    double a0 = 2.0 * M_PI * u01(b[1]), a1 = 2.0 * M_PI * u01(b[3]);
+    out[0] = r0 * cos(a0);
+    out[1] = r0 * sin(a0);
+    out[2] = r1 * cos(a1);
+}
+
+/* Engine pair force: same pair arithmetic as the reference (float, minimum
+ * image d -= L floor(d/L + 1/2)), per-species-pair cut distance
+ * s_ab = (s_a + s_b)/2 for a != b, sums in ascending partner index. */
+void or_eng_forces(int n, const float *pos, const int *type, float side, const float sigma[2], float *ff,
+                   float *pot, float *vir, int *nbr, uint64_t *nbr_hash) {
+    float side_inv = 1.0f / side;
+    float sig[2][2];
+    sig[0][0] = sigma[0]; sig[1][1] = sigma[1];
+    sig[0][1] = sig[1][0] = 0.5f * (sigma[0] + sigma[1]);
+    for (int m = 0; m < n; m++) {
+        float fx = 0, fy = 0, fz = 0, pm = 0, vm = 0;
+        int cnt = 0;
+        uint64_t h = 0;
+        for (int j = 0; j < n; j++) {
+            if (j == m) continue;
+            float s = sig[type[m]][type[j]], c2 = s * s;
+            float dx = pos[3 * j] - pos[3 * m], dy = pos[3 * j + 1] - pos[3 * m + 1], dz = pos[3 * j + 2] - pos[3 * m + 2];
+            dx -= side * floorf(side_inv * dx + 0.5f);
+            dy -= side * floorf(side_inv * dy + 0.5f);
+            dz -= side * floorf(side_inv * dz + 0.5f);
+            float d2 = dx * dx + dy * dy + dz * dz;
+            if (d2 < c2) {
+                float di = sqrtf(1.0f / d2), nf;
+                wca_modified(s, di, &pm, &nf);
+                float px = nf * di * dx, py = nf * di * dy, pz = nf * di * dz;
+                fx += px; fy += py; fz += pz;
+                vm -= 0.5f * (dx * px + dy * py + dz * pz);
+                cnt++;
+                h += ((uint64_t)(j + 1)) * 0x9E3779B97F4A7C15ULL;
+            }
+        }
+        ff[3 * m] = fx; ff[3 * m + 1] = fy; ff[3 * m + 2] = fz;
+        if (pot) pot[m] = pm;
+        if (vir) vir[m] = vm;
+        if (nbr) nbr[m] = cnt;
+        if (nbr_hash) nbr_hash[m] = h;
+    }
+}
+
+/* amplitude of the random displacement, update_ermak.cu:114 with the
+ * mobility mob in place of 1/sigma: (float) sqrt(2.0 * T * mob * dt). */
+float or_eng_amplitude(float temp, float mob, float dt) { return (float)sqrt(2.0 * temp * mob * dt); }
+
+/* Engine update.  Displacement d = (F*mob)*dt + amp*xi (float, two
+ * roundings per product as in the reference), then the position pair
+ * (hi, lo) absorbs d exactly (Knuth TwoSum + renormalisation), the periodic
+ * wrap subtracts L*floor(hi/L) the same way, and dsp += (double)d. */
+static void two_sum(float a, float b, float *s, float *e) {
+    float ss = a + b, bp = ss - a;
+    *e = (a - (ss - bp)) + (b - bp);
+    *s = ss;
+}
+void or_eng_update(int n, float *hi, float *lo, double *dsp, const float *ff, const int *type, float side,
+                   double dt_d, const float mob[2], const float amp[2], const float *noise) {
+    float dt = (float)dt_d, side_inv = 1.0f / side;
+    for (int m = 0; m < n; m++) {
+        int t = type[m];
+        for (int k = 0; k < 3; k++) {
+            float d = ff[3 * m + k] * mob[t] * dt + amp[t] * noise[3 * m + k];
+            float s, e;
+            two_sum(hi[3 * m + k], d, &s, &e);
+            float c = lo[3 * m + k] + e;
+            float h2 = s + c;
+            c = c - (h2 - s);
+            float kw = floorf(side_inv * h2);
+            if (kw != 0.0f) {
+                float s2, e2;
+                two_sum(h2, -(side * kw), &s2, &e2);
+                c = c + e2;
+                h2 = s2 + c;
+                c = c - (h2 - s2);
+            }
+            hi[3 * m + k] = h2;
+            lo[3 * m + k] = c;
+            dsp[3 * m + k] += (double)d;
+        }
+    }
+}
+
+void or_eng_fself_msd(int n, const double *d, double q, double *fs, double *msd) {
+    double sf = 0, sm = 0;
+    for (int i = 0; i < n; i++) {
+        double r2 = d[3 * i] * d[3 * i] + d[3 * i + 1] * d[3 * i + 1] + d[3 * i + 2] * d[3 * i + 2];
+        double r = sqrt(r2);
+        sm += r2;
+        sf += (r > 0) ? sin(q * r) / (q * r) : 1.0;
+    }
+    *fs = sf / n;
+    *msd = sm / n;
+}
