@@ -1,0 +1,150 @@
+// common.cuh -- device arithmetic shared by every kernel of libbd_aging_b200.
+//
+// Exactness rules.  Pair selection (cut-off test), cell indices and g(r) bins
+// must be bit-identical to the reference's host functions given identical
+// positions.  The reference host code rounds every product and sum separately
+// (no fused multiply-add on x86-64), so these helpers use the explicitly
+// rounded intrinsics __fmul_rn / __fadd_rn / __fsub_rn, which the compiler
+// never contracts into FMA.  The force arithmetic itself only has to agree to
+// a tolerance and is written in plain C so the compiler may fuse it.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace bd {
+
+// encabezados.h:25 and :30 (PI is 3.14159266f in the reference, sic)
+constexpr float kRefPi = 3.14159266f;
+constexpr float kEps = 1.0f;
+
+// device status word bits (OR-ed by kernels, read by the host after a call)
+enum : unsigned {
+    kStatCellOverflow = 1u,   // a cell or staging buffer exceeded its capacity
+    kStatNumeric = 2u,        // non-finite position
+    kStatArg = 4u,            // inconsistent arguments detected on device
+    kStatTimeout = 8u,        // a bounded wait expired
+};
+
+__device__ __forceinline__ void set_status(unsigned *st, unsigned bits) {
+    if (st) atomicOr(st, bits);
+}
+
+// ------------------------------------------------------------ minimum image
+// get_forces.cu:389-391: d -= side * floor(side_inv * d + 0.5f)  (float)
+__device__ __forceinline__ float min_image_f(float d, float side, float side_inv) {
+    return __fsub_rn(d, __fmul_rn(side, floorf(__fadd_rn(__fmul_rn(side_inv, d), 0.5f))));
+}
+// get_gder.cu:113-115: floorf(side_inv * d + 0.5) with the 0.5 added in
+// double and the sum narrowed to float (same value as the float sum: the
+// double sum is exact, so both are one correct rounding of it).
+__device__ __forceinline__ float min_image_gder(float d, float side, float side_inv) {
+    float t = __double2float_rn(__dadd_rn((double)__fmul_rn(side_inv, d), 0.5));
+    return __fsub_rn(d, __fmul_rn(side, floorf(t)));
+}
+// (dx*dx + dy*dy) + dz*dz, every operation rounded (reference host order)
+__device__ __forceinline__ float dist2_rn(float dx, float dy, float dz) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+}
+
+// ------------------------------------------------------------------ WCA pair
+// potential_wca_modified (potentials.cu:137-147) for a pair inside its cut
+// distance sigma: eps[(s/r)^12 - 2 (s/r)^6 + 1] with dist_inv = sqrt(1/dist2)
+// (get_forces.cu:397), pair force along d (get_forces.cu:403-405) and the
+// virial increment -0.5 d.f (get_forces.cu:413).
+struct PairOut {
+    float fx, fy, fz, pot, vir;
+};
+__device__ __forceinline__ PairOut wca_modified_pair(float sigma, float dist2, float dx, float dy, float dz) {
+    float dist_inv = __fsqrt_rn(__frcp_rn(dist2));
+    float sor = dist_inv * sigma;
+    float sor6 = sor * sor * sor;
+    sor6 = sor6 * sor6;
+    float sor12 = sor6 * sor6;
+    PairOut o;
+    o.pot = kEps * (sor12 - 2 * sor6 + 1);
+    float nf = -kEps * 12 * (sor12 - sor6) * dist_inv;
+    o.fx = nf * dist_inv * dx;
+    o.fy = nf * dist_inv * dy;
+    o.fz = nf * dist_inv * dz;
+    o.vir = -0.5f * (dx * o.fx + dy * o.fy + dz * o.fz);
+    return o;
+}
+
+// ------------------------------------------------------- counter-based RNG
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11, "Parallel random
+// numbers: as easy as 1, 2, 3"): ten rounds of two 32x32->64 multiplies with
+// a Weyl-sequence key schedule.  Stateless: the engine keys it on
+// (replica seed) and counts on (particle id, step, stream).
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+        k.x += 0x9E3779B9u;
+        k.y += 0xBB67AE85u;
+    }
+    return c;
+}
+// uniform in (0,1): (x >> 9) 2^-23 + 2^-24 = (2k+1) 2^-24 with 2k+1 < 2^24,
+// exact in float
+__device__ __forceinline__ float u01(uint32_t x) {
+    return __fmaf_rn((float)(x >> 9), 1.1920928955078125e-07f, 5.9604644775390625e-08f);
+}
+// Three N(0,1) values by the Box-Muller transform of two uniform pairs.
+__device__ __forceinline__ float3 gauss3(uint64_t seed, uint32_t id, uint64_t step, uint32_t stream) {
+    uint4 b = philox4x32_10(make_uint4(id, (uint32_t)step, (uint32_t)(step >> 32), stream),
+                            make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
+    float r0 = sqrtf(-2.0f * logf(u01(b.x)));
+    float r1 = sqrtf(-2.0f * logf(u01(b.z)));
+    float s0, c0;
+    sincospif(2.0f * u01(b.y), &s0, &c0);
+    float c1 = cospif(2.0f * u01(b.w));
+    return make_float3(r0 * c0, r0 * s0, r1 * c1);
+}
+
+// --------------------------------------------------- compensated position
+// Knuth's TwoSum: s + e == a + b exactly.
+__device__ __forceinline__ void two_sum(float a, float b, float &s, float &e) {
+    s = __fadd_rn(a, b);
+    float bp = __fsub_rn(s, a);
+    e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bp)), __fsub_rn(b, bp));
+}
+// Position carried as hi + lo (|lo| <= ulp(hi)/2).  Adds d exactly, then
+// wraps into the periodic box by subtracting side*floor(hi/side) the same
+// exact way.  hi stays in [0, side] (side itself only through rounding, as in
+// the reference, update_ermak.cu:139-141), which cell indexing clamps.
+__device__ __forceinline__ void advance_wrap(float &hi, float &lo, float d, float side, float side_inv) {
+    float s, e;
+    two_sum(hi, d, s, e);
+    float c = __fadd_rn(lo, e);
+    float h2 = __fadd_rn(s, c);
+    c = __fsub_rn(c, __fsub_rn(h2, s));
+    float kw = floorf(__fmul_rn(side_inv, h2));
+    if (kw != 0.0f) {
+        float s2, e2;
+        two_sum(h2, -__fmul_rn(side, kw), s2, e2);
+        c = __fadd_rn(c, e2);
+        h2 = __fadd_rn(s2, c);
+        c = __fsub_rn(c, __fsub_rn(h2, s2));
+    }
+    hi = h2;
+    lo = c;
+}
+
+// Temperature protocols, set_temp.cu:7-23, same float arithmetic (the
+// reference host code has no FMA; the intrinsics keep it that way).
+__host__ __device__ inline float temp_linear(float T0, float Tf, float t0, float tf, float t) {
+    if (t < t0) return T0;
+    if (t > tf) return Tf;
+#ifdef __CUDA_ARCH__
+    float m = __fdiv_rn(__fsub_rn(Tf, T0), __fsub_rn(tf, t0));
+    return __fadd_rn(T0, __fmul_rn(m, __fsub_rn(t, t0)));
+#else
+    volatile float m = (Tf - T0) / (tf - t0);
+    volatile float p = m * (t - t0);
+    return T0 + p;
+#endif
+}
+
+}  // namespace bd

@@ -1,0 +1,615 @@
+// engine.cu -- host driver of the batched replica engine (bd_engine_* ABI):
+// geometry, buffers, initial load, CUDA-graph stepping, observation passes,
+// export, and the batch g(r) kernel.
+#include "engine_kernels.cuh"
+
+namespace bd {
+
+// ------------------------------------------------------------- batch g(r)
+// get_gder_dev (get_gder.cu:69-127) for all four species pairs of one
+// replica in one pass over unordered pairs i < j: the forward distance
+// (r_i - r_j) counts for (type_i, type_j), the reverse one for (type_j,
+// type_i), recomputed when the minimum-image rounding can differ.  Big
+// particles come first, so i < j gives bb, bs and ss forward and bb, sb, ss
+// in reverse.
+constexpr int kGrTile = 1024;
+__device__ __forceinline__ int gr_bin(float dx, float dy, float dz, float side, float side_inv, float range,
+                                      float range2_hi, float bin_size, int nbins) {
+    dx = min_image_gder(dx, side, side_inv);
+    dy = min_image_gder(dy, side, side_inv);
+    dz = min_image_gder(dz, side, side_inv);
+    float d2 = dist2_rn(dx, dy, dz);
+    if (!(d2 <= range2_hi)) return -1;
+    float dist = __fsqrt_rn(d2);
+    if (!(dist < range)) return -1;
+    int bin = (int)__fdiv_rn(dist, bin_size);
+    if (bin == nbins) bin--;
+    return bin;
+}
+__global__ void __launch_bounds__(256) k_gr_batch(const float4 *__restrict__ snap, int n, int n_big, float side,
+                                                  float range, int nbins, int jchunk, unsigned long long *counts) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    float4 *tile = reinterpret_cast<float4 *>(smem);
+    unsigned *hist = reinterpret_cast<unsigned *>(tile + kGrTile);  // [4][nbins]
+    for (int b = threadIdx.x; b < 4 * nbins; b += blockDim.x) hist[b] = 0;
+    const float side_inv = __double2float_rn(1.0 / (double)side);
+    const float bin_size = __fdiv_rn(range, (float)nbins);
+    const float range2_hi = range * range * 1.00001f;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool vi = i < n;
+    float4 pi = vi ? snap[i] : make_float4(0, 0, 0, 0);
+    const int ti = i < n_big ? 0 : 1;
+    int j0 = max(blockIdx.y * jchunk, (int)(blockIdx.x * blockDim.x) + 1), j1 = min(n, (int)(blockIdx.y + 1) * jchunk);
+    __syncthreads();
+    for (int t0 = j0; t0 < j1; t0 += kGrTile) {
+        const int tn = min(kGrTile, j1 - t0);
+        __syncthreads();
+        for (int t = threadIdx.x; t < tn; t += blockDim.x) tile[t] = snap[t0 + t];
+        __syncthreads();
+        for (int t = 0; t < tn; t++) {
+            const int j = t0 + t;
+            const int tj = j < n_big ? 0 : 1;
+            int kf = -1, kr = -1;
+            if (vi && j > i) {
+                float4 pj = tile[t];
+                float dx = __fsub_rn(pi.x, pj.x), dy = __fsub_rn(pi.y, pj.y), dz = __fsub_rn(pi.z, pj.z);
+                int bf = gr_bin(dx, dy, dz, side, side_inv, range, range2_hi, bin_size, nbins);
+                bool sym = fabsf(__fmul_rn(side_inv, dx)) < 0.25f && fabsf(__fmul_rn(side_inv, dy)) < 0.25f &&
+                           fabsf(__fmul_rn(side_inv, dz)) < 0.25f;
+                int bb = sym ? bf : gr_bin(-dx, -dy, -dz, side, side_inv, range, range2_hi, bin_size, nbins);
+                if (bf >= 0) kf = (ti * 2 + tj) * nbins + bf;
+                if (bb >= 0) kr = (tj * 2 + ti) * nbins + bb;
+            }
+            unsigned s1 = __match_any_sync(0xffffffffu, kf);
+            if (kf >= 0 && (threadIdx.x & 31) == __ffs(s1) - 1) atomicAdd(&hist[kf], (unsigned)__popc(s1));
+            unsigned s2 = __match_any_sync(0xffffffffu, kr);
+            if (kr >= 0 && (threadIdx.x & 31) == __ffs(s2) - 1) atomicAdd(&hist[kr], (unsigned)__popc(s2));
+        }
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < 4 * nbins; b += blockDim.x)
+        if (hist[b]) atomicAdd(&counts[b], (unsigned long long)hist[b]);
+}
+
+}  // namespace bd
+
+using namespace bd;
+
+struct bd_engine {
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    int R = 0;
+    std::vector<bd_system_desc> desc;
+    std::vector<SysDev> sysh;
+    SysDev *d_sys = nullptr;
+    std::vector<int4> bricks_h;
+    int4 *d_bricks = nullptr;
+    int nbricks = 0;
+    int bx = 4, by = 4, bz = 4, cap = 16, threads = 128, smax = 0, mode = BD_MODE_PLAIN, cluster = 8;
+    size_t smem = 0;
+    long long C = 0, P = 0;
+    int *cnt[3] = {nullptr, nullptr, nullptr};
+    float4 *pos[3] = {nullptr, nullptr, nullptr};
+    int cur = 0;
+    float *lo[3] = {nullptr, nullptr, nullptr};
+    double *dsp[3] = {nullptr, nullptr, nullptr};
+    int *gid_of = nullptr, *rep_of_sid = nullptr, *rep_of_gid = nullptr;
+    double *x0 = nullptr, *obs = nullptr;
+    float4 *snap = nullptr;
+    int *nbr_count = nullptr;
+    unsigned long long *nbr_hash = nullptr;
+    curandState *cr = nullptr;
+    float *noise = nullptr;
+    unsigned *status = nullptr;
+    long long *d_ni = nullptr;
+    float *out_pos = nullptr, *out_raw = nullptr;
+    long long ni = 0, ni_first = 0;
+    int rng = BD_RNG_PHILOX;
+    unsigned rng_stream = 0;
+    float qmax = 6.2831853f;
+    bool loaded = false;
+    int graph_steps = 96;
+    cudaGraphExec_t gexec = nullptr;
+    int autotune = 0;
+    bool tuned = false;
+};
+
+namespace {
+
+int engine_status(bd_engine *e) {
+    unsigned bits = 0;
+    BD_CUDA_TRY(cudaMemcpyAsync(&bits, e->status, sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream));
+    BD_CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return status_from_bits(bits);
+}
+
+StepArgs make_args(bd_engine *e, int buf, int do_update) {
+    StepArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.sys = e->d_sys;
+    a.bricks = e->d_bricks;
+    a.nbricks = e->nbricks;
+    a.bx = e->bx; a.by = e->by; a.bz = e->bz;
+    a.cap = e->cap;
+    a.smax = e->smax;
+    a.cnt_in = e->cnt[buf % 3];
+    a.pos_in = e->pos[buf % 3];
+    a.cnt_out = e->cnt[(buf + 1) % 3];
+    a.pos_out = e->pos[(buf + 1) % 3];
+    a.cnt_clr = e->cnt[(buf + 2) % 3];
+    a.lo_x = e->lo[0]; a.lo_y = e->lo[1]; a.lo_z = e->lo[2];
+    a.dsp_x = e->dsp[0]; a.dsp_y = e->dsp[1]; a.dsp_z = e->dsp[2];
+    a.gid_of = e->gid_of;
+    a.x0 = e->x0;
+    a.snap = e->snap;
+    a.obs = e->obs;
+    a.nbr_count = e->nbr_count;
+    a.nbr_hash = e->nbr_hash;
+    a.curand_states = e->cr;
+    a.noise = e->noise;
+    a.status = e->status;
+    a.ni_first = e->ni_first;
+    a.qmax = e->qmax;
+    a.do_update = do_update;
+    a.rng_stream = e->rng_stream;
+    return a;
+}
+
+// Dynamic shared memory above 48 KB needs a per-kernel attribute; it is set
+// outside stream capture (launch_step_t with attr_only) before any graph is
+// recorded.
+template <int RNG, bool OBS, bool CENSUS>
+int launch_step_t(bd_engine *e, const StepArgs &a, int ni_off, bool attr_only = false) {
+    auto kern = k_step<RNG, OBS, CENSUS>;
+    if (attr_only) {
+        BD_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e->smem));
+        return BD_OK;
+    }
+    kern<<<e->nbricks, e->threads, e->smem, e->stream>>>(a, e->d_ni, ni_off);
+    BD_LAUNCH_CHECK();
+    return BD_OK;
+}
+
+int configure_kernels(bd_engine *e) {
+    StepArgs a;
+    std::memset(&a, 0, sizeof(a));
+    int rc = 0;
+#define BD_ATTR(R)                                                 \
+    rc |= launch_step_t<R, false, false>(e, a, 0, true);           \
+    rc |= launch_step_t<R, true, false>(e, a, 0, true);            \
+    rc |= launch_step_t<R, false, true>(e, a, 0, true);
+    BD_ATTR(kRngPhilox)
+    BD_ATTR(kRngCurand)
+    BD_ATTR(kRngNoise)
+#undef BD_ATTR
+    return rc ? BD_ERR_CUDA : BD_OK;
+}
+
+int launch_step(bd_engine *e, const StepArgs &a, int ni_off, bool obs, bool census) {
+    if (census) {
+        if (e->rng == BD_RNG_CURAND) return launch_step_t<kRngCurand, false, true>(e, a, ni_off);
+        if (e->rng == BD_RNG_NOISE) return launch_step_t<kRngNoise, false, true>(e, a, ni_off);
+        return launch_step_t<kRngPhilox, false, true>(e, a, ni_off);
+    }
+    if (obs) {
+        if (e->rng == BD_RNG_CURAND) return launch_step_t<kRngCurand, true, false>(e, a, ni_off);
+        if (e->rng == BD_RNG_NOISE) return launch_step_t<kRngNoise, true, false>(e, a, ni_off);
+        return launch_step_t<kRngPhilox, true, false>(e, a, ni_off);
+    }
+    if (e->rng == BD_RNG_CURAND) return launch_step_t<kRngCurand, false, false>(e, a, ni_off);
+    if (e->rng == BD_RNG_NOISE) return launch_step_t<kRngNoise, false, false>(e, a, ni_off);
+    return launch_step_t<kRngPhilox, false, false>(e, a, ni_off);
+}
+
+// one plain step (outside graphs): launch, advance the device counter
+int plain_step(bd_engine *e) {
+    StepArgs a = make_args(e, e->cur, 1);
+    int rc = launch_step(e, a, 0, false, false);
+    if (rc) return rc;
+    k_advance_counter<<<1, 1, 0, e->stream>>>(e->d_ni, 1);
+    BD_LAUNCH_CHECK();
+    e->cur = (e->cur + 1) % 3;
+    e->ni += 1;
+    return BD_OK;
+}
+
+int build_graph(bd_engine *e) {
+    if (e->gexec) return BD_OK;
+    cudaGraph_t g;
+    BD_CUDA_TRY(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = BD_OK;
+    for (int j = 0; j < e->graph_steps && rc == BD_OK; j++) {
+        StepArgs a = make_args(e, e->cur + j, 1);
+        rc = launch_step(e, a, j, false, false);
+    }
+    if (rc == BD_OK) k_advance_counter<<<1, 1, 0, e->stream>>>(e->d_ni, e->graph_steps);
+    cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+    if (rc) return rc;
+    BD_CUDA_TRY(ce);
+    BD_CUDA_TRY(cudaGraphInstantiate(&e->gexec, g, 0));
+    cudaGraphDestroy(g);
+    return BD_OK;
+}
+
+void free_engine(bd_engine *e) {
+    if (e->gexec) cudaGraphExecDestroy(e->gexec);
+    void *ptrs[] = {e->d_sys, e->d_bricks, e->cnt[0], e->cnt[1], e->cnt[2], e->pos[0], e->pos[1], e->pos[2],
+                    e->lo[0], e->lo[1], e->lo[2], e->dsp[0], e->dsp[1], e->dsp[2], e->gid_of, e->rep_of_sid,
+                    e->rep_of_gid, e->x0, e->obs, e->snap, e->nbr_count, e->nbr_hash, e->cr, e->noise,
+                    e->status, e->d_ni, e->out_pos, e->out_raw};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+}
+
+int setup_geometry(bd_engine *e) {
+    e->sysh.resize(e->R);
+    long long cell_base = 0, part_base = 0;
+    e->bricks_h.clear();
+    for (int r = 0; r < e->R; r++) {
+        const bd_system_desc &d = e->desc[r];
+        SysDev &S = e->sysh[r];
+        std::memset(&S, 0, sizeof(S));
+        if (d.n_big < 0 || d.n_sml < 0 || d.n_big + d.n_sml < 1 || !(d.side > 0) || !(d.sigma_big > 0) ||
+            !(d.sigma_sml > 0) || !(d.dt > 0))
+            return BD_ERR_ARG;
+        S.L = d.side;
+        S.Linv = 1.0f / d.side;
+        S.sig[0] = d.sigma_big;
+        S.sig[1] = 0.5f * (d.sigma_big + d.sigma_sml);  // get_forces.cu:441
+        S.sig[2] = d.sigma_sml;
+        for (int k = 0; k < 3; k++) S.cut2[k] = S.sig[k] * S.sig[k];
+        float rcmax = std::max(S.sig[0], std::max(S.sig[1], S.sig[2]));
+        int nc = (int)std::floor((double)d.side / ((double)rcmax * (1.0 + 1e-5)));
+        if (nc < 3) return BD_ERR_ARG;  // box too small for a 27-cell sweep
+        S.ncell = nc;
+        S.cinv = (float)nc / d.side;
+        S.cell_base = (int)cell_base;
+        S.n = d.n_big + d.n_sml;
+        S.n_big = d.n_big;
+        S.part_base = (int)part_base;
+        S.mob[0] = d.mob_big;
+        S.mob[1] = d.mob_sml;
+        S.dt = (float)d.dt;
+        S.dt_d = d.dt;
+        S.fcap = d.force_cap;
+        S.protocol = d.temp_protocol;
+        S.T0 = d.T0; S.Tf = d.Tf; S.t0 = d.t0; S.tf = d.tf; S.period = d.period;
+        S.seed = d.seed;
+        S.nbx = (nc + e->bx - 1) / e->bx;
+        S.nby = (nc + e->by - 1) / e->by;
+        S.nbz = (nc + e->bz - 1) / e->bz;
+        S.brick_base = (int)e->bricks_h.size();
+        for (int z = 0; z < S.nbz; z++)
+            for (int y = 0; y < S.nby; y++)
+                for (int x = 0; x < S.nbx; x++) e->bricks_h.push_back(make_int4(r, x * e->bx, y * e->by, z * e->bz));
+        cell_base += (long long)nc * nc * nc;
+        part_base += S.n;
+        if (cell_base > (1ll << 31) / e->cap || part_base >= (1ll << 31)) return BD_ERR_ARG;
+    }
+    e->C = cell_base;
+    e->P = part_base;
+    e->nbricks = (int)e->bricks_h.size();
+    const int nh = (e->bx + 2) * (e->by + 2) * (e->bz + 2);
+    e->smax = std::min(65535, std::max(256, 4 * nh));
+    e->smem = brick_smem_bytes(nh, e->smax);
+    if (e->smem > 227 * 1024) return BD_ERR_ARG;
+    return BD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void bd_engine_opts_default(bd_engine_opts *o) {
+    std::memset(o, 0, sizeof(*o));
+    o->rng = BD_RNG_PHILOX;
+    o->cell_capacity = 16;
+    o->mode = BD_MODE_AUTO;
+    o->cluster = 8;
+    o->graph_steps = 96;
+    o->qmax = 6.2831853f;
+}
+
+int bd_engine_create(const bd_system_desc *systems, int nsys, const bd_engine_opts *opts_in, bd_engine **out) {
+    if (!systems || nsys < 1 || !out) return BD_ERR_ARG;
+    *out = nullptr;
+    bd_engine_opts opts;
+    if (opts_in) opts = *opts_in; else bd_engine_opts_default(&opts);
+    bd_engine *e = new (std::nothrow) bd_engine();
+    if (!e) return BD_ERR_NOMEM;
+    if (cudaGetDevice(&e->dev) != cudaSuccess) { delete e; return BD_ERR_CUDA; }
+    e->R = nsys;
+    e->desc.assign(systems, systems + nsys);
+    e->rng = opts.rng;
+    if (e->rng < 0 || e->rng > 2) { delete e; return BD_ERR_ARG; }
+    e->cap = opts.cell_capacity > 0 ? opts.cell_capacity : 16;
+    if (opts.brick[0] > 0 && opts.brick[1] > 0 && opts.brick[2] > 0) {
+        e->bx = opts.brick[0]; e->by = opts.brick[1]; e->bz = opts.brick[2];
+    }
+    e->threads = opts.threads > 0 ? opts.threads : 128;
+    if (e->threads % 32 || e->threads > 256) { delete e; return BD_ERR_ARG; }
+    e->mode = opts.mode == BD_MODE_AUTO ? BD_MODE_PLAIN : opts.mode;
+    e->cluster = opts.cluster > 0 ? opts.cluster : 8;
+    e->graph_steps = opts.graph_steps > 0 ? ((opts.graph_steps + 2) / 3) * 3 : 96;
+    e->qmax = opts.qmax != 0.f ? opts.qmax : 6.2831853f;
+    e->ni = e->ni_first = opts.ni_start;
+    e->rng_stream = opts.rng_stream;
+    e->autotune = opts.autotune;
+    int rc = setup_geometry(e);
+    if (rc) { delete e; return rc; }
+#define ALLOC(ptr, bytes)                                                    \
+    do {                                                                     \
+        if (cudaMalloc((void **)&(ptr), (bytes)) != cudaSuccess) {          \
+            free_engine(e);                                                  \
+            return BD_ERR_NOMEM;                                             \
+        }                                                                    \
+    } while (0)
+    if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) { delete e; return BD_ERR_CUDA; }
+    const size_t P = (size_t)e->P, C = (size_t)e->C;
+    ALLOC(e->d_sys, sizeof(SysDev) * e->R);
+    ALLOC(e->d_bricks, sizeof(int4) * e->nbricks);
+    for (int k = 0; k < 3; k++) {
+        ALLOC(e->cnt[k], sizeof(int) * C);
+        ALLOC(e->pos[k], sizeof(float4) * C * e->cap);
+        ALLOC(e->lo[k], sizeof(float) * P);
+        ALLOC(e->dsp[k], sizeof(double) * P);
+    }
+    ALLOC(e->gid_of, sizeof(int) * P);
+    ALLOC(e->rep_of_sid, sizeof(int) * P);
+    ALLOC(e->rep_of_gid, sizeof(int) * P);
+    ALLOC(e->x0, sizeof(double) * 3 * P);
+    ALLOC(e->snap, sizeof(float4) * P);
+    ALLOC(e->obs, sizeof(double) * kObsCount * e->R);
+    ALLOC(e->status, 256);
+    ALLOC(e->d_ni, sizeof(long long));
+    if (e->rng == BD_RNG_CURAND) ALLOC(e->cr, sizeof(curandState) * P);
+    if (e->rng == BD_RNG_NOISE) ALLOC(e->noise, sizeof(float) * 3 * P);
+#undef ALLOC
+    cudaMemcpyAsync(e->d_sys, e->sysh.data(), sizeof(SysDev) * e->R, cudaMemcpyHostToDevice, e->stream);
+    cudaMemcpyAsync(e->d_bricks, e->bricks_h.data(), sizeof(int4) * e->nbricks, cudaMemcpyHostToDevice, e->stream);
+    cudaMemsetAsync(e->status, 0, 256, e->stream);
+    cudaMemcpyAsync(e->d_ni, &e->ni, sizeof(long long), cudaMemcpyHostToDevice, e->stream);
+    std::vector<int> rog(P);
+    for (int r = 0; r < e->R; r++)
+        for (int i = 0; i < e->sysh[r].n; i++) rog[e->sysh[r].part_base + i] = r;
+    cudaMemcpyAsync(e->rep_of_gid, rog.data(), sizeof(int) * P, cudaMemcpyHostToDevice, e->stream);
+    if (e->rng == BD_RNG_CURAND) {
+        k_curand_setup<<<div_up((long)P, 128), 128, 0, e->stream>>>(e->cr, e->d_sys, e->rep_of_gid, (int)P);
+    }
+    if (configure_kernels(e) != BD_OK) {
+        free_engine(e);
+        return BD_ERR_CUDA;
+    }
+    if (cudaStreamSynchronize(e->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+        free_engine(e);
+        return BD_ERR_CUDA;
+    }
+    *out = e;
+    return BD_OK;
+}
+
+int bd_engine_destroy(bd_engine *e) {
+    if (!e) return BD_ERR_ARG;
+    cudaStreamSynchronize(e->stream);
+    free_engine(e);
+    return BD_OK;
+}
+
+int bd_engine_get_info(const bd_engine *e, bd_engine_info *info) {
+    if (!e || !info) return BD_ERR_ARG;
+    std::memset(info, 0, sizeof(*info));
+    info->nsys = e->R;
+    info->n_particles = e->P;
+    info->n_cells = e->C;
+    info->brick[0] = e->bx; info->brick[1] = e->by; info->brick[2] = e->bz;
+    info->threads = e->threads;
+    info->cell_capacity = e->cap;
+    info->staging_capacity = e->smax;
+    info->mode = e->mode;
+    info->cluster = e->cluster;
+    info->smem_bytes = e->smem;
+    info->next_step = e->ni;
+    return BD_OK;
+}
+
+int bd_engine_get_stream(const bd_engine *e, void **stream) {
+    if (!e || !stream) return BD_ERR_ARG;
+    *stream = (void *)e->stream;
+    return BD_OK;
+}
+
+int bd_engine_set_positions(bd_engine *e, const float *pos) {
+    if (!e || !pos) return BD_ERR_ARG;
+    const size_t P = (size_t)e->P;
+    // storage order: replica, brick, cell within brick, reference index
+    std::vector<long long> key(P);
+    std::vector<int> order(P);
+    for (int r = 0; r < e->R; r++) {
+        const SysDev &S = e->sysh[r];
+        for (int i = 0; i < S.n; i++) {
+            size_t g = (size_t)S.part_base + i;
+            float x = pos[3 * g], y = pos[3 * g + 1], z = pos[3 * g + 2];
+            if (!(x >= 0.f && x <= S.L && y >= 0.f && y <= S.L && z >= 0.f && z <= S.L)) return BD_ERR_ARG;
+            int ix = std::min(std::max((int)(x * S.cinv), 0), S.ncell - 1);
+            int iy = std::min(std::max((int)(y * S.cinv), 0), S.ncell - 1);
+            int iz = std::min(std::max((int)(z * S.cinv), 0), S.ncell - 1);
+            long long b = (ix / e->bx) + (long long)S.nbx * ((iy / e->by) + (long long)S.nby * (iz / e->bz));
+            long long c = (ix % e->bx) + e->bx * ((iy % e->by) + e->by * (iz % e->bz));
+            key[g] = (((long long)r << 40) | (b << 16) | c);
+            order[g] = (int)g;
+        }
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key[a] < key[b]; });
+    std::vector<float4> staged(P);
+    std::vector<int> gid_of(P), rep_of_sid(P);
+    for (size_t sid = 0; sid < P; sid++) {
+        int g = order[sid];
+        int r = 0;
+        // replica of g
+        {
+            int lo = 0, hi = e->R - 1;
+            while (lo < hi) {
+                int mid = (lo + hi + 1) / 2;
+                if (e->sysh[mid].part_base <= g) lo = mid; else hi = mid - 1;
+            }
+            r = lo;
+        }
+        const SysDev &S = e->sysh[r];
+        unsigned type = (g - S.part_base) < S.n_big ? 0u : 1u;
+        unsigned w = (unsigned)sid | (type << 31);
+        float wf;
+        std::memcpy(&wf, &w, 4);
+        staged[sid] = make_float4(pos[3 * (size_t)g], pos[3 * (size_t)g + 1], pos[3 * (size_t)g + 2], wf);
+        gid_of[sid] = g;
+        rep_of_sid[sid] = r;
+    }
+    float4 *d_staged = nullptr;
+    BD_CUDA_TRY(cudaMalloc(&d_staged, sizeof(float4) * P));
+    cudaMemcpyAsync(d_staged, staged.data(), sizeof(float4) * P, cudaMemcpyHostToDevice, e->stream);
+    cudaMemcpyAsync(e->gid_of, gid_of.data(), sizeof(int) * P, cudaMemcpyHostToDevice, e->stream);
+    cudaMemcpyAsync(e->rep_of_sid, rep_of_sid.data(), sizeof(int) * P, cudaMemcpyHostToDevice, e->stream);
+    for (int k = 0; k < 3; k++) {
+        cudaMemsetAsync(e->cnt[k], 0, sizeof(int) * e->C, e->stream);
+        cudaMemsetAsync(e->lo[k], 0, sizeof(float) * P, e->stream);
+        cudaMemsetAsync(e->dsp[k], 0, sizeof(double) * P, e->stream);
+    }
+    cudaMemsetAsync(e->status, 0, 256, e->stream);
+    e->cur = 0;
+    k_load<<<div_up((long)P, 256), 256, 0, e->stream>>>(d_staged, (int)P, e->rep_of_sid, e->d_sys, e->cnt[0],
+                                                        e->pos[0], e->cap, e->x0, e->gid_of, e->status);
+    cudaError_t le = cudaGetLastError();
+    cudaStreamSynchronize(e->stream);
+    cudaFree(d_staged);
+    if (le != cudaSuccess) return BD_ERR_CUDA;
+    if (e->gexec) { cudaGraphExecDestroy(e->gexec); e->gexec = nullptr; }
+    e->loaded = true;
+    return engine_status(e);
+}
+
+int bd_engine_run(bd_engine *e, long long nsteps) {
+    if (!e || nsteps < 0) return BD_ERR_ARG;
+    if (!e->loaded) return BD_ERR_STATE;
+    if (e->rng == BD_RNG_NOISE && nsteps > 1) return BD_ERR_ARG;  // one injected step at a time
+    while (nsteps > 0) {
+        if (nsteps >= e->graph_steps && e->rng != BD_RNG_NOISE) {
+            int rc = build_graph(e);
+            if (rc) return rc;
+            BD_CUDA_TRY(cudaGraphLaunch(e->gexec, e->stream));
+            e->ni += e->graph_steps;  // cur unchanged: graph_steps is a multiple of 3
+            nsteps -= e->graph_steps;
+        } else {
+            int rc = plain_step(e);
+            if (rc) return rc;
+            nsteps -= 1;
+        }
+    }
+    return engine_status(e);
+}
+
+int bd_engine_observe(bd_engine *e, bd_observables *out) {
+    if (!e || !out) return BD_ERR_ARG;
+    if (!e->loaded) return BD_ERR_STATE;
+    BD_CUDA_TRY(cudaMemsetAsync(e->obs, 0, sizeof(double) * kObsCount * e->R, e->stream));
+    StepArgs a = make_args(e, e->cur, 0);
+    int rc = launch_step(e, a, 0, true, false);
+    if (rc) return rc;
+    std::vector<double> h((size_t)kObsCount * e->R);
+    BD_CUDA_TRY(cudaMemcpyAsync(h.data(), e->obs, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, e->stream));
+    rc = engine_status(e);
+    for (int r = 0; r < e->R; r++) {
+        const SysDev &S = e->sysh[r];
+        const double *o = h.data() + (size_t)r * kObsCount;
+        const int nb = S.n_big, ns = S.n - S.n_big;
+        bd_observables &v = out[r];
+        v.energy_big = nb ? 0.5 * o[kObsPotBig] / nb : 0.0;
+        v.energy_sml = ns ? 0.5 * o[kObsPotSml] / ns : 0.0;
+        v.virial = o[kObsVir];
+        v.msd_big = nb ? o[kObsMsdBig] / nb : 0.0;
+        v.msd_sml = ns ? o[kObsMsdSml] / ns : 0.0;
+        v.fself_big = nb ? o[kObsFsBig] / nb : 0.0;
+        v.nbr_pairs = 0.0;
+        // temp_set after the last completed step ni-1: time = dt (1 + (float)(ni-1))
+        const bd_system_desc &d = e->desc[r];
+        float t = (float)(d.dt * (1.0 + (float)(e->ni - 1)));
+        float T = d.T0;
+        if (e->ni > e->ni_first) {
+            if (d.temp_protocol == BD_PROTOCOL_LINEAR) T = bd_calculate_temp_linear(d.T0, d.Tf, d.t0, d.tf, t);
+            else if (d.temp_protocol == BD_PROTOCOL_SINE) T = bd_calculate_temp_sine(d.T0, d.Tf, d.t0, d.tf, d.period, t);
+        }
+        v.temperature = T;
+    }
+    return rc;
+}
+
+int bd_engine_get_positions(bd_engine *e, float *pos_host, float *raw_host) {
+    if (!e) return BD_ERR_ARG;
+    if (!e->loaded) return BD_ERR_STATE;
+    const size_t P = (size_t)e->P;
+    if (!e->out_pos) {
+        if (cudaMalloc(&e->out_pos, sizeof(float) * 3 * P) != cudaSuccess) return BD_ERR_NOMEM;
+        if (cudaMalloc(&e->out_raw, sizeof(float) * 3 * P) != cudaSuccess) return BD_ERR_NOMEM;
+    }
+    k_export<<<div_up(e->C, 128), 128, 0, e->stream>>>(e->cnt[e->cur], e->pos[e->cur], (int)e->C, e->cap, e->gid_of,
+                                                       e->x0, e->dsp[0], e->dsp[1], e->dsp[2], e->out_pos,
+                                                       e->out_raw, e->snap);
+    BD_LAUNCH_CHECK();
+    if (pos_host) BD_CUDA_TRY(cudaMemcpyAsync(pos_host, e->out_pos, sizeof(float) * 3 * P, cudaMemcpyDeviceToHost, e->stream));
+    if (raw_host) BD_CUDA_TRY(cudaMemcpyAsync(raw_host, e->out_raw, sizeof(float) * 3 * P, cudaMemcpyDeviceToHost, e->stream));
+    return engine_status(e);
+}
+
+int bd_engine_gder(bd_engine *e, int nbins, float range, unsigned long long *counts_host) {
+    if (!e || !counts_host || nbins < 1 || nbins > 4096 || !(range > 0)) return BD_ERR_ARG;
+    if (!e->loaded) return BD_ERR_STATE;
+    k_export<<<div_up(e->C, 128), 128, 0, e->stream>>>(e->cnt[e->cur], e->pos[e->cur], (int)e->C, e->cap, e->gid_of,
+                                                       e->x0, e->dsp[0], e->dsp[1], e->dsp[2], nullptr, nullptr,
+                                                       e->snap);
+    BD_LAUNCH_CHECK();
+    unsigned long long *d_counts = nullptr;
+    const size_t per = (size_t)4 * nbins;
+    BD_CUDA_TRY(cudaMalloc(&d_counts, sizeof(unsigned long long) * per * e->R));
+    cudaMemsetAsync(d_counts, 0, sizeof(unsigned long long) * per * e->R, e->stream);
+    const size_t sm = kGrTile * sizeof(float4) + per * sizeof(unsigned);
+    cudaFuncSetAttribute(k_gr_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    const int jchunk = 8192;
+    for (int r = 0; r < e->R; r++) {
+        const SysDev &S = e->sysh[r];
+        dim3 grid(div_up(S.n, 256), div_up(S.n, jchunk));
+        k_gr_batch<<<grid, 256, sm, e->stream>>>(e->snap + S.part_base, S.n, S.n_big, S.L, range, nbins, jchunk,
+                                                 d_counts + per * r);
+    }
+    cudaError_t le = cudaGetLastError();
+    cudaMemcpyAsync(counts_host, d_counts, sizeof(unsigned long long) * per * e->R, cudaMemcpyDeviceToHost, e->stream);
+    cudaStreamSynchronize(e->stream);
+    cudaFree(d_counts);
+    if (le != cudaSuccess) return BD_ERR_CUDA;
+    return engine_status(e);
+}
+
+int bd_engine_set_noise(bd_engine *e, const float *noise_host) {
+    if (!e || !noise_host || e->rng != BD_RNG_NOISE) return BD_ERR_ARG;
+    BD_CUDA_TRY(cudaMemcpyAsync(e->noise, noise_host, sizeof(float) * 3 * e->P, cudaMemcpyHostToDevice, e->stream));
+    return BD_OK;
+}
+
+int bd_engine_census(bd_engine *e, int *nbr_count, unsigned long long *nbr_hash) {
+    if (!e || !nbr_count || !nbr_hash) return BD_ERR_ARG;
+    if (!e->loaded) return BD_ERR_STATE;
+    if (!e->nbr_count) {
+        if (cudaMalloc(&e->nbr_count, sizeof(int) * e->P) != cudaSuccess) return BD_ERR_NOMEM;
+        if (cudaMalloc(&e->nbr_hash, sizeof(unsigned long long) * e->P) != cudaSuccess) return BD_ERR_NOMEM;
+    }
+    BD_CUDA_TRY(cudaMemsetAsync(e->obs, 0, sizeof(double) * kObsCount * e->R, e->stream));
+    StepArgs a = make_args(e, e->cur, 0);
+    a.nbr_count = e->nbr_count;
+    a.nbr_hash = e->nbr_hash;
+    int rc = launch_step(e, a, 0, false, true);
+    if (rc) return rc;
+    BD_CUDA_TRY(cudaMemcpyAsync(nbr_count, e->nbr_count, sizeof(int) * e->P, cudaMemcpyDeviceToHost, e->stream));
+    BD_CUDA_TRY(cudaMemcpyAsync(nbr_hash, e->nbr_hash, sizeof(unsigned long long) * e->P, cudaMemcpyDeviceToHost, e->stream));
+    return engine_status(e);
+}
+
+}  // extern "C"

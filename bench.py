@@ -1,0 +1,416 @@
+#!/usr/bin/env python
+"""Throughput of the Ermak-McCammon time step (cell list -> WCA pair forces ->
+stochastic update) of the bidisperse WCA mixture, in particle-steps/s.
+
+Workload (default "aging"): the aging quench of N = 32768 (16384 big sigma 1.4,
+16384 small sigma 1.0 in WCA units), phi = 0.58, T 1.0 -> 0.1 instantaneous
+jump, dt = 1e-5, run as R independent replicas in one batched engine
+(batched vs plain is the metric; the plain single-replica engine is timed
+beside it).  Inputs are synthetic: uniform random positions relaxed by 2000
+capped-force steps on the GPU (the reference ships no configuration
+generator).  One bench "step" = `--md-steps` time steps of every replica.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs its own replicas (replicas only: the path does
+not shard, there is no collective on the data path); value = all ranks'
+particle-steps / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s on 1 B200, batched vs plain, at matched g(r)/F_s error"
+ALG_BYTES_PER_PARTICLE_STEP = 96  # FP32 position + remainder (24 B) and FP64 displacement (24 B), read + write
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="aging", choices=["aging", "batched", "large", "small"])
+    ap.add_argument("--replicas", type=int, default=64)
+    ap.add_argument("--md-steps", type=int, default=960)
+    ap.add_argument("--no-extras", action="store_true", help="skip plain/e2e/reference-CUDA/CPU legs")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ workloads
+def workload_systems(name, replicas, rank):
+    """Returns (systems, description dict). Seeds differ per rank."""
+    from bd_aging_b200 import configs as CF
+    from bd_aging_b200 import lib as B
+    sb, ss = float(CF.SIGMA_BIG), float(CF.SIGMA_SML)
+    rng = np.random.default_rng(1000 + rank)
+    out = []
+    if name == "aging":
+        nb = ns = 16384
+        side = float(np.float32(CF.side_from_phi(nb, ns, 0.58)))
+        for r in range(replicas):
+            out.append(B.System(n_big=nb, n_sml=ns, side=side, sigma_big=sb, sigma_sml=ss, dt=1e-5, T0=1.0, Tf=0.1,
+                                t0=0.0, tf=1e-30, protocol="linear", seed=1 + r + 100000 * rank))
+        desc = {"workload": "aging quench N=32768 phi=0.58 T 1.0->0.1 dt=1e-5, %d replicas batched" % replicas,
+                "n_per_replica": 32768, "replicas": replicas, "phi": 0.58}
+    elif name == "batched":
+        for r in range(256):
+            n = int(rng.integers(500, 8001)) // 2 * 2
+            phi = float(rng.uniform(0.50, 0.60))
+            tfin = float(rng.uniform(0.05, 1.0))
+            side = float(np.float32(CF.side_from_phi(n // 2, n // 2, phi)))
+            out.append(B.System(n_big=n // 2, n_sml=n // 2, side=side, sigma_big=sb, sigma_sml=ss, dt=1e-5, T0=1.0,
+                                Tf=tfin, t0=0.0, tf=1e-30, protocol="linear", seed=7 + r + 100000 * rank))
+        desc = {"workload": "256 ragged replicas N in [500,8000] phi in [0.50,0.60] T_final in [0.05,1.0] dt=1e-5",
+                "replicas": 256}
+    elif name == "large":
+        nb = ns = 524288
+        side = float(np.float32(CF.side_from_phi(nb, ns, 0.58)))
+        out.append(B.System(n_big=nb, n_sml=ns, side=side, sigma_big=sb, sigma_sml=ss, dt=1e-5, T0=0.2,
+                            protocol="const", seed=3 + 100000 * rank))
+        desc = {"workload": "large single system N=1048576 phi=0.58 T=0.2 dt=1e-5", "replicas": 1}
+    else:
+        nb = ns = 500
+        side = float(np.float32(CF.side_from_phi(nb, ns, 0.50)))
+        out.append(B.System(n_big=nb, n_sml=ns, side=side, sigma_big=sb, sigma_sml=ss, dt=2e-5, T0=1.0,
+                            protocol="const", seed=1 + 100000 * rank))
+        desc = {"workload": "small N=1000 phi=0.50 T=1.0 dt=2e-5 single replica", "replicas": 1}
+    return out, desc
+
+
+def relaxed_positions(systems, seed):
+    """Uniform random positions relaxed by 2000 capped-force steps on the GPU
+    (Philox stream 1), all replicas at once."""
+    from bd_aging_b200 import configs as CF
+    from bd_aging_b200 import lib as B
+    import dataclasses
+    pos = np.concatenate([CF.uniform_config(s.n_big, s.n_sml, s.side, seed + k) for k, s in enumerate(systems)])
+    relax = [dataclasses.replace(s, dt=1e-4, protocol="const", T0=1.0, force_cap=100.0) for s in systems]
+    e = B.Engine(relax, rng_stream=1)
+    e.set_positions(pos)
+    e.run(2000)
+    p, _ = e.get_positions()
+    e.close()
+    return p
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for ln in open(self.path):
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, nm in enumerate(names):
+                if r[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic_per_particle_step():
+    """DRAM bytes per particle-step of the step kernel from the committed ncu
+    summary (profiles/k_step_aging.md, line 'dram_bytes_per_particle_step: X')."""
+    p = os.path.join(ROOT, "profiles", "k_step_aging.md")
+    if not os.path.exists(p):
+        return None
+    for ln in open(p):
+        if ln.strip().startswith("dram_bytes_per_particle_step:"):
+            try:
+                return float(ln.split(":")[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# ------------------------------------------------------------------ legs
+def cuda_time(engine, fn, iters):
+    import torch
+    s = torch.cuda.ExternalStream(engine.stream_handle())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(s)
+    for _ in range(iters):
+        fn()
+    e1.record(s)
+    e1.synchronize()
+    return e0.elapsed_time(e1)  # ms
+
+
+def cpu_baseline(seconds=12.0):
+    """Reference host implementation (oracle/_ref) on one N=32768 phi=0.58
+    replica, single thread (the reference's *_hst functions keep state in
+    static locals), bounded sample."""
+    from oracle import oracle as O
+    from bd_aging_b200 import configs as CF
+    if not O.ref_available():
+        return None
+    nb = ns = 16384
+    side = float(np.float32(CF.side_from_phi(nb, ns, 0.58)))
+    pos = CF.lattice_config(nb, ns, side, 99, jitter=0.05)
+    p = O.setup_params(side, nb, ns, float(CF.SIGMA_BIG), float(CF.SIGMA_SML), ntags=(16, 16), nbins=400,
+                       rng=side / 2, dt=1e-5, T0=1.0)
+    run = O.RefHostRun(p, pos)
+    t = time.perf_counter()
+    run.run(1, 1.0, 0.1, 0.0, 1e-30, 1e-5)
+    one = max(time.perf_counter() - t, 1e-4)
+    n = max(1, int(seconds / one))
+    t = time.perf_counter()
+    run.run(n, 1.0, 0.1, 0.0, 1e-30, 1e-5)
+    el = time.perf_counter() - t
+    return {"value": 32768 * n / el, "unit": "particle-steps/s", "cores": 1, "kind": "reference",
+            "sample": "%d steps of one N=32768 phi=0.58 replica, reference host loop (oracle/_ref)" % n}
+
+
+def reference_cuda(steps=200):
+    """The reference's own CUDA kernels (oracle/_ref/libref.so, built from the
+    reference sources for sm_100a) in its main.cu step order, one N=32768
+    phi=0.58 system, ntags 16."""
+    from oracle import oracle as O
+    from bd_aging_b200 import configs as CF
+    import ctypes as C
+    if not O.ref_available():
+        return None
+    nb = ns = 16384
+    side = float(np.float32(CF.side_from_phi(nb, ns, 0.58)))
+    pos = relaxed_positions_single(nb, ns, side)
+    p = O.setup_params(side, nb, ns, float(CF.SIGMA_BIG), float(CF.SIGMA_SML), ntags=(16, 16), nbins=400,
+                       rng=side / 2, dt=1e-5, T0=1.0)
+    ob, os_ = np.zeros((nb, 3), np.float32), np.zeros((ns, 3), np.float32)
+    wb, ws = np.zeros_like(ob), np.zeros_like(os_)
+    ms = C.c_float(0)
+    rc = O.ref_lib().ref_cuda_run(C.byref(p), pos[:nb].copy(), pos[nb:].copy(), 0, 20, 1, 1.0, 0.1, 0.0, 1e-30,
+                                  1e-5, ob, os_, wb, ws, C.byref(ms))
+    rc = O.ref_lib().ref_cuda_run(C.byref(p), pos[:nb].copy(), pos[nb:].copy(), 0, steps, 1, 1.0, 0.1, 0.0, 1e-30,
+                                  1e-5, ob, os_, wb, ws, C.byref(ms))
+    if rc != 0:
+        return {"error": "reference CUDA run returned %d" % rc}
+    return {"value": 32768 * steps / (ms.value / 1e3), "unit": "particle-steps/s", "steps": steps,
+            "ms_per_step": ms.value / steps}
+
+
+_RELAXED_CACHE = {}
+
+
+def relaxed_positions_single(nb, ns, side):
+    from bd_aging_b200 import configs as CF
+    from bd_aging_b200 import lib as B
+    key = (nb, ns, side)
+    if key not in _RELAXED_CACHE:
+        s = B.System(n_big=nb, n_sml=ns, side=side, sigma_big=float(CF.SIGMA_BIG), sigma_sml=float(CF.SIGMA_SML),
+                     dt=1e-5, T0=1.0, protocol="const", seed=1)
+        _RELAXED_CACHE[key] = relaxed_positions([s], 4242)
+    return _RELAXED_CACHE[key]
+
+
+def run_ours(args):
+    import torch
+    from bd_aging_b200 import lib as B
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    systems, desc = workload_systems(args.workload, args.replicas, rank)
+    pos = relaxed_positions(systems, 777 + rank)
+    P = sum(s.n for s in systems)
+    S = args.md_steps
+    eng = B.Engine(systems, graph_steps=96)
+    eng.set_positions(pos)
+    info = eng.info()
+    for _ in range(args.warmup):
+        eng.run(S)
+    clocks = ClockSampler(local)
+    clocks.start()
+    if dist:
+        dist.barrier()
+    ms = cuda_time(eng, lambda: eng.run(S), args.steps)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    ck = clocks.stop()
+    total_ps = P * S * args.steps * world
+    value = total_ps / (ms / 1e3)
+    launches = S * args.steps
+    avg_launch_s = (ms / 1e3) / launches
+    peak, peak_kind = measured_peak_hbm()
+    achieved = ALG_BYTES_PER_PARTICLE_STEP * P / avg_launch_s / 1e9
+    tpp = profile_traffic_per_particle_step()
+    line = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 forces, f32+compensation positions, f64 displacement",
+            "data": "synthetic: uniform random positions relaxed by 2000 capped-force steps (GPU)",
+            "config": dict(desc, md_steps_per_bench_step=S, mobility="reference 1/sigma",
+                           l2="inputs larger than L2" if P * 112 > 126e6 else "state fits in L2",
+                           brick=list(info.brick), threads=info.threads, cell_capacity=info.cell_capacity),
+            "gpu_launches": int(launches + args.steps * math.ceil(S / 96)),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "alg_bytes_per_launch": ALG_BYTES_PER_PARTICLE_STEP * P,
+                         "traffic": (tpp * P) if tpp else None},
+            "clocks": ck}
+    if rank == 0 and world == 1 and not args.no_extras:
+        # plain single-replica engine, same system
+        s1 = systems[0]
+        e1 = B.Engine([s1], graph_steps=96)
+        e1.set_positions(pos[: s1.n])
+        e1.run(S)
+        k1 = max(3, args.steps)
+        ms1 = cuda_time(e1, lambda: e1.run(S), k1)
+        plain = s1.n * S * k1 / (ms1 / 1e3)
+        e1.close()
+        line["plain"] = {"value": plain, "unit": "particle-steps/s", "replicas": 1}
+        line["batched_over_plain"] = value / plain
+        # end to end through the C ABI with host buffers
+        out_pos = np.zeros((P, 3), np.float32)
+
+        def e2e_step():
+            eng.set_positions(pos)
+            eng.run(S)
+            out_pos[:] = eng.get_positions()[0]
+        e2e_step()
+        ms2 = cuda_time(eng, e2e_step, max(2, args.steps // 2))
+        k2 = max(2, args.steps // 2)
+        line["e2e"] = {"value": P * S * k2 / (ms2 / 1e3), "unit": "particle-steps/s",
+                       "h2d_bytes_per_step": P * (16 + 4 + 4), "d2h_bytes_per_step": P * 24}
+        try:
+            line["reference_cuda"] = reference_cuda()
+            if line["reference_cuda"] and "value" in line["reference_cuda"]:
+                line["batched_over_reference_cuda"] = value / line["reference_cuda"]["value"]
+        except Exception as ex:  # reported, never fatal for the bench line
+            line["reference_cuda"] = {"error": str(ex)[:200]}
+        line["cpu_baseline"] = cpu_baseline()
+    eng.close()
+    if dist:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+# ------------------------------------------------------------ reference arm
+def _ref_worker(args_tuple):
+    nsteps, reps, seed = args_tuple
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    from bd_aging_b200 import configs as CF
+    nb = ns = 16384
+    side = float(np.float32(CF.side_from_phi(nb, ns, 0.58)))
+    pos = CF.lattice_config(nb, ns, side, seed, jitter=0.05)
+    p = O.setup_params(side, nb, ns, float(CF.SIGMA_BIG), float(CF.SIGMA_SML), ntags=(16, 16), nbins=400,
+                       rng=side / 2, dt=1e-5, T0=1.0)
+    run = O.RefHostRun(p, pos, seed)
+    t = time.perf_counter()
+    for _ in range(reps):
+        run.run(nsteps, 1.0, 0.1, 0.0, 1e-30, 1e-5)
+    return time.perf_counter() - t
+
+
+def run_reference(args):
+    """The reference's own CPU implementation (host functions compiled from its
+    sources, oracle/_ref) on every host core: one independent N=32768 replica
+    per process (its functions are not reentrant), each bench step a bounded
+    sample of 2 time steps per replica."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref.so not built"}))
+        return
+    import multiprocessing as mp
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except Exception:
+        cores = os.cpu_count() or 1
+    per = 2
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        pool.map(_ref_worker, [(per, max(1, args.warmup // 3), 11 + k) for k in range(cores)])
+        t = time.perf_counter()
+        times = pool.map(_ref_worker, [(per, args.steps, 11 + k) for k in range(cores)])
+        wall = time.perf_counter() - t
+    total = 32768 * per * args.steps * cores
+    value = total / wall
+    line = {"metric": METRIC, "impl": "reference", "value": value, "unit": "particle-steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: jittered lattice at phi=0.58",
+            "config": {"workload": "aging quench N=32768 phi=0.58 T 1.0->0.1 dt=1e-5, one replica per host core",
+                       "replicas": cores, "md_steps_per_bench_step": per},
+            "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores, "kind": "reference",
+                             "sample": "%d replicas x %d steps per bench step, reference host loop" % (cores, per)},
+            "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

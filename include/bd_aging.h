@@ -185,6 +185,102 @@ int bd_cv3d_calculate_vector(bd_cv3d *cv);
 int bd_cv3d_get_vector(const bd_cv3d *cv, float *out);
 int bd_cv3d_destroy(bd_cv3d *cv);
 
+/* ---- batched replica engine ------------------------------------------------
+ * Replaces the reference time loop (main.cu:494-588, one system per process,
+ * 18 kernel launches and 3 device synchronisations per step, configurations
+ * run one after another, main.cu:213) with one fused launch per step over
+ * all replicas, or one persistent launch per chunk of steps. */
+typedef struct bd_engine bd_engine;
+
+#define BD_PROTOCOL_LINEAR 0   /* calculate_temp_linear, set_temp.cu:7-12 */
+#define BD_PROTOCOL_SINE 1     /* calculate_temp_sine, set_temp.cu:14-23 */
+#define BD_PROTOCOL_CONST 2    /* T = T0 throughout */
+
+#define BD_RNG_PHILOX 0   /* counter-based Philox4x32-10 + Box-Muller (default) */
+#define BD_RNG_CURAND 1   /* the reference's cuRAND XORWOW stream: big seeded with
+                             seed, small with seed+1, subsequence = index within
+                             the species (main.cu:478-484) */
+#define BD_RNG_NOISE 2    /* caller-supplied N(0,1) values (bd_engine_set_noise) */
+
+#define BD_MODE_AUTO 0
+#define BD_MODE_PLAIN 1       /* one launch per step, steps captured in CUDA graphs */
+#define BD_MODE_PERSISTENT 2  /* one launch per chunk; thread-block clusters own
+                                 replicas and synchronise between steps */
+
+typedef struct bd_system_desc {
+    int n_big, n_sml;          /* particles 0..n_big-1 are big (main.cu:387-393) */
+    float side;                /* cubic periodic box side */
+    float sigma_big, sigma_sml;/* reference `sigma`: the WCA cut distance s; the
+                                  big-small pair uses (s_b + s_s)/2 */
+    float mob_big, mob_sml;    /* mobilities; the reference uses 1/sigma
+                                  (update_ermak.cu:106-114) */
+    double dt;
+    int temp_protocol;         /* BD_PROTOCOL_* */
+    float T0, Tf, t0, tf, period;
+    unsigned long long seed;   /* RNG key of this replica (idum for BD_RNG_CURAND) */
+    float force_cap;           /* > 0: |F| capped (initial-configuration relaxation) */
+} bd_system_desc;
+
+typedef struct bd_engine_opts {
+    int rng;                   /* BD_RNG_* */
+    int cell_capacity;         /* slots per cell (0 = 16) */
+    int brick[3];              /* cells per brick (0 = autotune / default) */
+    int threads;               /* CTA size (0 = default) */
+    int mode;                  /* BD_MODE_* */
+    int cluster;               /* CTAs per cluster in persistent mode (0 = 8) */
+    int autotune;              /* 1: time brick/CTA shapes at first run */
+    int graph_steps;           /* steps per captured CUDA graph (0 = 96) */
+    float qmax;                /* wave number of the built-in F_s observable */
+    long long ni_start;        /* reference step index of the first update
+                                  (-ntrans, main.cu:407 and 494) */
+    unsigned rng_stream;       /* Philox stream number (0 dynamics, 1 relaxation) */
+} bd_engine_opts;
+
+typedef struct bd_observables {
+    double energy_big, energy_sml; /* (1/N) sum 0.5 pot_i per species (main.cu:627-631) */
+    double virial;                 /* sum of per-particle virials (main.cu:801-803) */
+    double msd_big, msd_sml;       /* mean |r - r(step 0)|^2 (main.cu:776-792), FP64 */
+    double fself_big;              /* F_s(qmax) of the big particles (fself.cu), FP64 */
+    double nbr_pairs;              /* interacting ordered pairs (census only) */
+    double temperature;            /* temp_set after the last completed step */
+} bd_observables;
+
+typedef struct bd_engine_info {
+    int nsys;
+    long long n_particles, n_cells;
+    int brick[3], threads, cell_capacity, staging_capacity, mode, cluster;
+    size_t smem_bytes;
+    long long next_step;          /* reference ni of the next update */
+} bd_engine_info;
+
+void bd_engine_opts_default(bd_engine_opts *opts);
+/* Geometry + buffers for nsys replicas.  Box sides must hold >= 3 cells of
+ * the largest cut distance. */
+int bd_engine_create(const bd_system_desc *systems, int nsys, const bd_engine_opts *opts, bd_engine **out);
+int bd_engine_destroy(bd_engine *e);
+int bd_engine_get_info(const bd_engine *e, bd_engine_info *info);
+/* The CUDA stream all engine work is issued on (for caller-side events). */
+int bd_engine_get_stream(const bd_engine *e, void **stream);
+/* Host positions of all replicas, float3 per particle, replica after replica,
+ * each in the reference order (big first).  Resets displacements. */
+int bd_engine_set_positions(bd_engine *e, const float *pos_host);
+/* Advance every replica by nsteps reference steps. */
+int bd_engine_run(bd_engine *e, long long nsteps);
+/* Observables of the current state (the reference's sample step: forces of
+ * the positions after the last update).  out: nsys entries. */
+int bd_engine_observe(bd_engine *e, bd_observables *out);
+/* Wrapped (rr) and unwrapped (rr_raw) positions, float3 per particle in the
+ * set_positions order.  Either pointer may be NULL. */
+int bd_engine_get_positions(bd_engine *e, float *pos_host, float *raw_host);
+/* g(r) counts of the current state: counts_host[nsys][4][nbins] (bb, bs, sb,
+ * ss ordered pairs, get_gder.cu arithmetic), exact integers. */
+int bd_engine_gder(bd_engine *e, int nbins, float range, unsigned long long *counts_host);
+/* BD_RNG_NOISE: N(0,1) values for the next step, 3 per particle (set_positions order). */
+int bd_engine_set_noise(bd_engine *e, const float *noise_host);
+/* Interacting partners of every particle and a hash of their indices (the
+ * neighbour set), from the engine's own pair selection.  Host outputs. */
+int bd_engine_census(bd_engine *e, int *nbr_count, unsigned long long *nbr_hash);
+
 #ifdef __cplusplus
 }
 #endif

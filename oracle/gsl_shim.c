@@ -12,15 +12,35 @@ const gsl_rng_type *gsl_rng_mt19937 = &shim_mt;
 gsl_rng *gsl_rng_alloc(const gsl_rng_type *t) {
     (void)t;
     gsl_rng *r = (gsl_rng *)calloc(1, sizeof(gsl_rng));
+    gsl_rng_set(r, 0);
     return r;
 }
-void gsl_rng_set(gsl_rng *r, unsigned long seed) { (void)seed; r->pos = 0; }
+void gsl_rng_set(gsl_rng *r, unsigned long seed) {
+    r->pos = 0;
+    r->s = 0x9E3779B97F4A7C15ULL ^ (unsigned long long)seed;
+    if (!r->s) r->s = 1;
+    r->has_spare = 0;
+}
+/* xorshift64* (Vigna 2016) -> uniform in (-1, 1) */
+static double shim_u11(gsl_rng *r) {
+    r->s ^= r->s >> 12; r->s ^= r->s << 25; r->s ^= r->s >> 27;
+    unsigned long long x = r->s * 2685821657736338717ULL;
+    return ((double)(x >> 11) + 0.5) * (2.0 / 9007199254740992.0) - 1.0;
+}
 void gsl_rng_free(gsl_rng *r) { free(r); }
 void gsl_shim_rng_set_noise(gsl_rng *r, const double *noise, long n) {
     r->noise = noise; r->n = n; r->pos = 0;
 }
 double gsl_ran_gaussian(gsl_rng *r, double sigma) {
-    if (!r->noise || r->pos >= r->n) {
+    if (!r->noise) { /* Marsaglia polar method */
+        if (r->has_spare) { r->has_spare = 0; return sigma * r->spare; }
+        double u, v, q;
+        do { u = shim_u11(r); v = shim_u11(r); q = u * u + v * v; } while (q >= 1.0 || q == 0.0);
+        double f = sqrt(-2.0 * log(q) / q);
+        r->spare = v * f; r->has_spare = 1;
+        return sigma * u * f;
+    }
+    if (r->pos >= r->n) {
         fprintf(stderr, "gsl shim: injected noise buffer exhausted (%ld)\n", r->pos);
         abort();
     }

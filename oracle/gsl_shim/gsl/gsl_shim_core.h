@@ -7,7 +7,9 @@
  *
  *  - gsl_rng / gsl_ran_gaussian: return sigma * (next value of an injected
  *    noise buffer), so that the reference update and the CUDA engine consume
- *    identical N(0,1) draws in parity tests.
+ *    identical N(0,1) draws in parity tests.  Without a buffer the shim draws
+ *    its own normals (xorshift64* + Marsaglia polar method) so that the
+ *    reference's host time loop can be timed with its RNG cost included.
  *  - gsl_linalg_SV_decomp: one-sided Jacobi SVD in double (own code).  The
  *    reference only uses the pseudo-inverse V diag(1/w) U^T, which does not
  *    depend on the SVD algorithm beyond rounding.
@@ -23,7 +25,7 @@ typedef struct { size_t size; double *data; } gsl_vector;
 typedef struct { size_t size1, size2; double *data; } gsl_matrix;
 
 typedef struct { const char *name; } gsl_rng_type;
-typedef struct { const double *noise; long n, pos; } gsl_rng;
+typedef struct { const double *noise; long n, pos; unsigned long long s; int has_spare; double spare; } gsl_rng;
 
 extern const gsl_rng_type *gsl_rng_mt19937;
 

@@ -409,8 +409,8 @@ void or_eng_uniform_bits(uint64_t seed, uint32_t id, uint64_t step, uint32_t str
     uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
     or_philox4x32_10(ctr, key, out);
 }
-/* uniform in (0,1): (x >> 8) * 2^-24 + 2^-25 (exact in float) */
-static double u01(uint32_t x) { return (double)(x >> 8) * (1.0 / 16777216.0) + (1.0 / 33554432.0); }
+/* uniform in (0,1): (x >> 9) * 2^-23 + 2^-24 (exact in float) */
+static double u01(uint32_t x) { return (double)(x >> 9) * (1.0 / 8388608.0) + (1.0 / 16777216.0); }
 void or_eng_gauss3(uint64_t seed, uint32_t id, uint64_t step, uint32_t stream, double out[3]) {
     uint32_t b[4];
     or_eng_uniform_bits(seed, id, step, stream, b);

@@ -136,6 +136,9 @@ def ref_lib():
         L.ref_cuda_run.restype = C.c_int
         L.ref_cuda_gder.argtypes = [P, _f32p, _f32p, _f32p]
         L.ref_cuda_gder.restype = C.c_int
+        L.ref_hst_run.argtypes = [P] + [_f32p] * 10 + [_i32p] * 4 + [C.c_long, C.c_long] + [C.c_float] * 4 + \
+            [C.c_double, C.c_ulong]
+        L.ref_hst_run.restype = C.c_int
         _ref = L
     return _ref
 
@@ -249,3 +252,30 @@ def cv3d_solve(ata, atb, dtype=np.float32):
         aux = (u.T @ np.asarray(atb[c], dtype)) * winv
         acc += v @ aux
     return (acc / 3).astype(dtype)
+
+
+class RefHostRun:
+    """The reference's host time loop (oracle/_ref ref_hst_run) on one system:
+    CPU baseline and reference arm of bench.py."""
+
+    def __init__(self, p: Parametros, pos: np.ndarray, seed: int = 1):
+        self.p = p
+        nb, ns = p.ngrain_big, p.ngrain_sml
+        self.rb = np.ascontiguousarray(pos[:nb], np.float32).copy()
+        self.rs = np.ascontiguousarray(pos[nb:], np.float32).copy()
+        self.rawb, self.raws = self.rb.copy(), self.rs.copy()
+        self.ffb, self.ffs = np.zeros_like(self.rb), np.zeros_like(self.rs)
+        self.vb, self.pb = np.zeros(nb, np.float32), np.zeros(nb, np.float32)
+        self.vs, self.ps = np.zeros(ns, np.float32), np.zeros(ns, np.float32)
+        ncb3, ncs3 = p.ncell_big ** 3, p.ncell_sml ** 3
+        self.nob, self.cb = np.zeros(ncb3, np.int32), np.zeros(ncb3 * p.ntags_big, np.int32)
+        self.nos, self.cs = np.zeros(ncs3, np.int32), np.zeros(ncs3 * p.ntags_sml, np.int32)
+        self.ni = 0
+        self.seed = seed
+
+    def run(self, nsteps, T0, Tf, t0, tf, dt):
+        rc = ref_lib().ref_hst_run(C.byref(self.p), self.rb, self.rs, self.rawb, self.raws, self.ffb, self.ffs,
+                                   self.vb, self.vs, self.pb, self.ps, self.nob, self.cb, self.nos, self.cs,
+                                   nsteps, self.ni, T0, Tf, t0, tf, dt, self.seed)
+        self.ni += nsteps
+        return rc

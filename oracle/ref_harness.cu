@@ -68,3 +68,49 @@ void ref_cv3d_get_vector(void *h, float *out) { ((Contracting_Vector3D *)h)->get
 void ref_cv3d_destroy(void *h) { delete (Contracting_Vector3D *)h; }
 
 }  // extern "C"
+
+extern "C" {
+/* The reference's host time loop, in the order of the HOST branches of
+ * main.cu:509-574 (update_ermak_hst x2, temperature, set_vec_int_hst +
+ * cell_locate_hst x2, set_vec_float*_hst, get_forces_same_hst x2,
+ * get_forces_diff_hst x2).  The HOST driver itself does not compile
+ * (main.cu:323); its functions do, and are called here unchanged.  Noise:
+ * the GSL stand-in's own normals.  rb/rs are advanced in place; ff/vir/pot
+ * are the caller's work arrays.  Returns 0. */
+int ref_hst_run(const parametros *p_in, float *rb, float *rs, float *rawb, float *raws, float *ffb, float *ffs,
+                float *vb, float *vs, float *pb, float *ps, int *nocup_b, int *cell_b, int *nocup_s, int *cell_s,
+                long nsteps, long ni_start, float T0, float Tf, float t0, float tf, double dt, unsigned long seed) {
+    parametros pars = *p_in;
+    gsl_rng *r = gsl_rng_alloc(gsl_rng_mt19937);
+    gsl_rng_set(r, seed);
+    const int nb = pars.ngrain_big, ns = pars.ngrain_sml;
+    const int ncb3 = pars.ncell_big * pars.ncell_big * pars.ncell_big;
+    const int ncs3 = pars.ncell_sml * pars.ncell_sml * pars.ncell_sml;
+    float3 zero; zero.x = zero.y = zero.z = 0.0f;
+    for (long k = 0; k < nsteps; k++) {
+        long ni = ni_start + k;
+        update_ermak_hst('b', (float3 *)rb, (float3 *)rawb, (float3 *)ffb, r, pars);
+        update_ermak_hst('s', (float3 *)rs, (float3 *)raws, (float3 *)ffs, r, pars);
+        float time = dt * (1.0 + (float)ni);
+        pars.temp_set = calculate_temp_linear(T0, Tf, t0, tf, time);
+        set_vec_int_hst(nocup_b, ncb3, 0);
+        set_vec_int_hst(cell_b, ncb3 * pars.ntags_big, -1);
+        cell_locate_hst('b', (float3 *)rb, nocup_b, cell_b, pars);
+        set_vec_int_hst(nocup_s, ncs3, 0);
+        set_vec_int_hst(cell_s, ncs3 * pars.ntags_sml, -1);
+        cell_locate_hst('s', (float3 *)rs, nocup_s, cell_s, pars);
+        set_vec_float3_hst((float3 *)ffb, nb, zero);
+        set_vec_float_hst(vb, nb, 0.0);
+        set_vec_float_hst(pb, nb, 0.0);
+        set_vec_float3_hst((float3 *)ffs, ns, zero);
+        set_vec_float_hst(vs, ns, 0.0);
+        set_vec_float_hst(ps, ns, 0.0);
+        get_forces_same_hst('b', (float3 *)rb, (float3 *)ffb, vb, pb, nocup_b, cell_b, pars);
+        get_forces_same_hst('s', (float3 *)rs, (float3 *)ffs, vs, ps, nocup_s, cell_s, pars);
+        get_forces_diff_hst('b', 's', (float3 *)rb, (float3 *)ffb, (float3 *)rs, vb, pb, nocup_s, cell_s, pars);
+        get_forces_diff_hst('s', 'b', (float3 *)rs, (float3 *)ffs, (float3 *)rb, vs, ps, nocup_b, cell_b, pars);
+    }
+    gsl_rng_free(r);
+    return 0;
+}
+}  // extern "C"

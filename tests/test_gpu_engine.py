@@ -1,0 +1,138 @@
+"""GPU parity of the batched replica engine against the oracle: neighbour
+sets (exact), one step with injected noise, observables, g(r) counts (exact),
+batched == plain bit identity, error paths."""
+import numpy as np
+import pytest
+
+from bd_aging_b200 import configs as CF
+from bd_aging_b200 import lib as B
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+SB, SS = float(CF.SIGMA_BIG), float(CF.SIGMA_SML)
+
+
+def system(nb, ns, phi, seed, **kw):
+    side = float(np.float32(CF.side_from_phi(nb, ns, phi)))
+    pos = CF.lattice_config(nb, ns, side, seed)
+    s = B.System(n_big=nb, n_sml=ns, side=side, sigma_big=SB, sigma_sml=SS, dt=kw.pop("dt", 1e-4), seed=seed, **kw)
+    return s, pos
+
+
+def types_of(s):
+    return np.array([0] * s.n_big + [1] * s.n_sml, np.int32)
+
+
+@pytest.mark.parametrize("nb,ns,phi,brick", [(150, 150, 0.45, None), (60, 240, 0.30, (2, 2, 2)),
+                                             (2000, 2000, 0.55, None), (2000, 2000, 0.55, (8, 4, 2)),
+                                             (700, 300, 0.5, (3, 5, 2))])
+def test_neighbour_sets_bit_exact(nb, ns, phi, brick):
+    s, pos = system(nb, ns, phi, 21)
+    e = B.Engine([s], brick=brick)
+    e.set_positions(pos)
+    cnt, hsh = e.census()
+    _, _, _, nbr, h = O.eng_forces(pos, types_of(s), s.side, SB, SS)
+    np.testing.assert_array_equal(cnt, nbr)
+    np.testing.assert_array_equal(hsh, h)
+    e.close()
+
+
+def test_one_step_with_injected_noise_matches_oracle():
+    s, pos = system(1500, 1500, 0.52, 4, T0=0.7)
+    e = B.Engine([s], rng="noise")
+    e.set_positions(pos)
+    noise = np.random.default_rng(9).standard_normal((s.n, 3)).astype(np.float32)
+    e.set_noise(noise)
+    e.run(1)
+    hi, raw = e.get_positions()
+    ff, _, _, _, _ = O.eng_forces(pos, types_of(s), s.side, SB, SS)
+    mob = np.array([np.float32(1) / np.float32(SB), np.float32(1) / np.float32(SS)], np.float32)
+    L = O.oracle_lib()
+    amp = np.array([L.or_eng_amplitude(0.7, float(mob[0]), np.float32(s.dt)),
+                    L.or_eng_amplitude(0.7, float(mob[1]), np.float32(s.dt))], np.float32)
+    ohi, olo, odsp = pos.copy(), np.zeros_like(pos), np.zeros(pos.shape, np.float64)
+    L.or_eng_update(s.n, ohi, olo, odsp, ff, types_of(s), s.side, s.dt, mob, amp, noise)
+    # forces are summed in another order (cells vs index), so positions agree
+    # to float rounding of the drift term
+    d = np.abs(hi - ohi)
+    d = np.minimum(d, s.side - d)
+    assert d.max() < 2e-6, d.max()
+    np.testing.assert_allclose(raw, (pos.astype(np.float64) + odsp).astype(np.float32), atol=2e-6)
+
+
+def test_observables_match_oracle():
+    s, pos = system(1200, 1800, 0.5, 8, T0=0.5)
+    e = B.Engine([s])
+    e.set_positions(pos)
+    ob = e.observe()[0]
+    _, pot, vir, _, _ = O.eng_forces(pos, types_of(s), s.side, SB, SS)
+    assert ob["energy_big"] == pytest.approx(0.5 * pot[:s.n_big].astype(np.float64).sum() / s.n_big, rel=1e-5)
+    assert ob["energy_sml"] == pytest.approx(0.5 * pot[s.n_big:].astype(np.float64).sum() / s.n_sml, rel=1e-5)
+    assert ob["virial"] == pytest.approx(vir.astype(np.float64).sum(), rel=1e-5)
+    assert ob["msd_big"] == 0.0 and ob["fself_big"] == 1.0
+    # after steps: MSD/F_s from the FP64 displacement equal the raw positions'
+    e.run(50)
+    ob = e.observe()[0]
+    _, raw = e.get_positions()
+    d = raw[: s.n_big].astype(np.float64) - pos[: s.n_big]
+    assert ob["msd_big"] == pytest.approx((d ** 2).sum(1).mean(), rel=1e-4)
+
+
+def test_gder_counts_exact_against_oracle():
+    s, pos = system(900, 1100, 0.5, 13)
+    e = B.Engine([s])
+    e.set_positions(pos)
+    nbins, rng_ = 150, s.side / 2
+    got = e.gder(nbins, rng_)[0]
+    p = O.setup_params(s.side, s.n_big, s.n_sml, SB, SS, nbins=nbins, rng=rng_)
+    ref = O.gder_counts(p, pos[: s.n_big], pos[s.n_big:])
+    np.testing.assert_array_equal(got, ref)
+
+
+def test_batched_equals_plain_bit_identical():
+    specs = [(300, 300, 0.5, 1), (1000, 700, 0.55, 2), (150, 450, 0.45, 3)]
+    systems, poss = zip(*[system(*sp, T0=1.0) for sp in specs])
+    eb = B.Engine(list(systems))
+    eb.set_positions(np.concatenate(poss))
+    eb.run(200)
+    pb, rb = eb.get_positions()
+    for k, (s, p) in enumerate(zip(systems, poss)):
+        e1 = B.Engine([s])
+        e1.set_positions(p)
+        e1.run(200)
+        p1, r1 = e1.get_positions()
+        sl = slice(eb.offsets[k], eb.offsets[k + 1])
+        np.testing.assert_array_equal(pb[sl], p1)
+        np.testing.assert_array_equal(rb[sl], r1)
+
+
+def test_graph_and_single_steps_agree():
+    s, pos = system(800, 800, 0.5, 5)
+    e1 = B.Engine([s], graph_steps=96)
+    e1.set_positions(pos)
+    e1.run(96 + 5)
+    e2 = B.Engine([s], graph_steps=96)
+    e2.set_positions(pos)
+    for _ in range(101):
+        e2.run(1)
+    np.testing.assert_array_equal(e1.get_positions()[0], e2.get_positions()[0])
+
+
+def test_cell_capacity_overflow_raises():
+    s, pos = system(400, 400, 0.55, 6)
+    with pytest.raises(B.BDError) as ei:
+        e = B.Engine([s], cell_capacity=1)
+        e.set_positions(pos)
+        e.run(3)
+    assert ei.value.code == 3
+
+
+def test_nan_temperature_of_instant_quench_is_reported():
+    # t0 == tf == 0 (run-fself.sh:30-31) gives T = NaN at t == 0 in the
+    # reference (set_temp.cu:10-11); the next update turns positions into NaN.
+    s, pos = system(300, 300, 0.45, 7, T0=1.0, Tf=0.25, t0=0.0, tf=0.0, protocol="linear")
+    e = B.Engine([s], ni_start=-10)
+    e.set_positions(pos)
+    with pytest.raises(B.BDError) as ei:
+        e.run(12)
+    assert ei.value.code == 9
