@@ -85,8 +85,8 @@ struct bd_engine {
     std::vector<int4> bricks_h;
     int4 *d_bricks = nullptr;
     int nbricks = 0;
-    int bx = 4, by = 4, bz = 4, cap = 16, threads = 128, smax = 0, mode = BD_MODE_PLAIN, cluster = 8;
-    size_t smem = 0;
+    int bx = 4, by = 4, bz = 3, cap = 16, threads = 128, smax = 0, mode = BD_MODE_PLAIN, cluster = 8;
+    size_t smem = 0, smem_census = 0;
     long long C = 0, P = 0;
     int *cnt[3] = {nullptr, nullptr, nullptr};
     float4 *pos[3] = {nullptr, nullptr, nullptr};
@@ -162,10 +162,11 @@ template <int RNG, bool OBS, bool CENSUS>
 int launch_step_t(bd_engine *e, const StepArgs &a, int ni_off, bool attr_only = false) {
     auto kern = k_step<RNG, OBS, CENSUS>;
     if (attr_only) {
-        BD_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e->smem));
+        BD_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(CENSUS ? e->smem_census : e->smem)));
         return BD_OK;
     }
-    kern<<<e->nbricks, e->threads, e->smem, e->stream>>>(a, e->d_ni, ni_off);
+    kern<<<e->nbricks, e->threads, CENSUS ? e->smem_census : e->smem, e->stream>>>(a, e->d_ni, ni_off);
     BD_LAUNCH_CHECK();
     return BD_OK;
 }
@@ -292,9 +293,10 @@ int setup_geometry(bd_engine *e) {
     e->P = part_base;
     e->nbricks = (int)e->bricks_h.size();
     const int nh = (e->bx + 2) * (e->by + 2) * (e->bz + 2);
-    e->smax = std::min(65535, std::max(256, 4 * nh));
-    e->smem = brick_smem_bytes(nh, e->smax);
-    if (e->smem > 227 * 1024) return BD_ERR_ARG;
+    e->smax = std::min(65535, std::max(256, (7 * nh) / 2));
+    e->smem = brick_smem_bytes(nh, e->smax, e->threads);
+    e->smem_census = e->smem;
+    if (e->smem_census > 227 * 1024) return BD_ERR_ARG;
     return BD_OK;
 }
 
@@ -329,7 +331,7 @@ int bd_engine_create(const bd_system_desc *systems, int nsys, const bd_engine_op
         e->bx = opts.brick[0]; e->by = opts.brick[1]; e->bz = opts.brick[2];
     }
     e->threads = opts.threads > 0 ? opts.threads : 128;
-    if (e->threads % 32 || e->threads > 256) { delete e; return BD_ERR_ARG; }
+    if (e->threads % 32 || e->threads > 192) { delete e; return BD_ERR_ARG; }  // k_step launch bounds
     e->mode = opts.mode == BD_MODE_AUTO ? BD_MODE_PLAIN : opts.mode;
     e->cluster = opts.cluster > 0 ? opts.cluster : 8;
     e->graph_steps = opts.graph_steps > 0 ? ((opts.graph_steps + 2) / 3) * 3 : 96;

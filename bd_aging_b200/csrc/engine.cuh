@@ -52,6 +52,9 @@ enum ObsField {
 
 enum RngMode { kRngPhilox = 0, kRngCurand = 1, kRngNoise = 2 };
 
+// candidates of one home cell held in registers per chunk (4 per lane)
+constexpr int kMaxCand = 128;
+
 struct StepArgs {
     const SysDev *sys;
     const int4 *bricks;  // (replica, ox, oy, oz)

@@ -104,266 +104,9 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
     return s;  // valid in thread 0
 }
 
-// shared-memory carve for a brick with nh halo cells and smax staged particles
-struct BrickSmem {
-    int *start, *hstart, *gc, *home;
-    unsigned char *code;
-    float4 *sp;
-    double *red;
-    int *tmp;
-    float *amp;
-};
-__host__ __device__ inline size_t brick_smem_bytes(int nh, int smax) {
-    size_t b = 0;
-    b += (size_t)(nh + 1) * 4 * 2;        // start, hstart
-    b += (size_t)nh * 4;                  // gc
-    b += (size_t)smax * 4;                // home
-    b += ((size_t)nh + 15) & ~(size_t)15; // code
-    b = (b + 15) & ~(size_t)15;
-    b += (size_t)smax * 16;               // sp
-    b += 32 * 8 + 64 * 4 + 16;            // red, tmp, amp
-    return b;
-}
-__device__ inline BrickSmem carve(unsigned char *base, int nh, int smax) {
-    BrickSmem s;
-    unsigned char *p = base;
-    s.start = (int *)p; p += (size_t)(nh + 1) * 4;
-    s.hstart = (int *)p; p += (size_t)(nh + 1) * 4;
-    s.gc = (int *)p; p += (size_t)nh * 4;
-    s.home = (int *)p; p += (size_t)smax * 4;
-    s.code = p; p += ((size_t)nh + 15) & ~(size_t)15;
-    p = (unsigned char *)(((uintptr_t)p + 15) & ~(uintptr_t)15);
-    s.sp = (float4 *)p; p += (size_t)smax * 16;
-    s.red = (double *)p; p += 32 * 8;
-    s.tmp = (int *)p; p += 64 * 4;
-    s.amp = (float *)p;
-    return s;
-}
-
-// ------------------------------------------------------------- the step
-template <int RNG, bool OBS, bool CENSUS>
-__device__ void process_brick(const StepArgs &a, int bidx, long long ni, unsigned char *smem_raw) {
-    const int4 br = a.bricks[bidx];
-    const SysDev &S = a.sys[br.x];
-    const int nc = S.ncell;
-    const int ox = br.y, oy = br.z, oz = br.w;
-    const int wx = min(a.bx, nc - ox), wy = min(a.by, nc - oy), wz = min(a.bz, nc - oz);
-    const int hx = wx + 2, hy = wy + 2, hz = wz + 2, nh = hx * hy * hz;
-    BrickSmem sm = carve(smem_raw, (a.bx + 2) * (a.by + 2) * (a.bz + 2), a.smax);
-    const int tid = threadIdx.x, T = blockDim.x;
-    const float L = S.L;
-
-    if (tid == 0) {
-        float Tm = step_temperature(S, ni, a.ni_first);
-        sm.amp[0] = amplitude(Tm, S.mob[0], S.dt);
-        sm.amp[1] = amplitude(Tm, S.mob[1], S.dt);
-    }
-    // 1. halo cells: global index, clamped count, periodic shift code
-    for (int h = tid; h < nh; h += T) {
-        int lx = h % hx, ly = (h / hx) % hy, lz = h / (hx * hy);
-        int gx = ox + lx - 1, gy = oy + ly - 1, gz = oz + lz - 1;
-        int sx = 0, sy = 0, sz = 0;
-        if (gx < 0) { gx += nc; sx = 1; } else if (gx >= nc) { gx -= nc; sx = -1; }
-        if (gy < 0) { gy += nc; sy = 1; } else if (gy >= nc) { gy -= nc; sy = -1; }
-        if (gz < 0) { gz += nc; sz = 1; } else if (gz >= nc) { gz -= nc; sz = -1; }
-        int gc = S.cell_base + gx + nc * (gy + nc * gz);
-        int c = __ldcg(a.cnt_in + gc);
-        if (c > a.cap) { set_status(a.status, kStatCellOverflow); c = a.cap; }
-        bool home = lx >= 1 && lx <= wx && ly >= 1 && ly <= wy && lz >= 1 && lz <= wz;
-        sm.gc[h] = gc;
-        sm.start[h] = c;
-        sm.hstart[h] = home ? c : 0;
-        sm.code[h] = (unsigned char)((sx + 1) | ((sy + 1) << 2) | ((sz + 1) << 4));
-    }
-    __syncthreads();
-    block_scan2(sm.start, sm.hstart, nh, sm.tmp);
-    const int M = sm.start[nh], MH = sm.hstart[nh];
-    if (M > a.smax) {  // staging capacity exceeded: flag and leave the brick
-        if (tid == 0) set_status(a.status, kStatCellOverflow);
-        return;
-    }
-    // 2. stage positions; sort each cell by storage id; list home particles
-    for (int h = tid; h < nh; h += T) {
-        const int st = sm.start[h], c = sm.start[h + 1] - st;
-        const float4 *src = a.pos_in + (size_t)sm.gc[h] * a.cap;
-        for (int k = 0; k < c; k++) {
-            float4 v = __ldcg(src + k);
-            unsigned key = __float_as_uint(v.w) & 0x7fffffffu;
-            int j = st + k - 1;
-            while (j >= st && (__float_as_uint(sm.sp[j].w) & 0x7fffffffu) > key) { sm.sp[j + 1] = sm.sp[j]; j--; }
-            sm.sp[j + 1] = v;
-        }
-        const int hs = sm.hstart[h];
-        if (sm.hstart[h + 1] > hs)
-            for (int k = 0; k < c; k++) sm.home[hs + k] = (st + k) | (h << 16);
-    }
-    __syncthreads();
-
-    // 3. forces + update per home particle
-    const float c2bb = S.cut2[0], c2bs = S.cut2[1], c2ss = S.cut2[2];
-    const float sgbb = S.sig[0], sgbs = S.sig[1], sgss = S.sig[2];
-    double acc_pb = 0, acc_ps = 0, acc_v = 0, acc_mb = 0, acc_ms = 0, acc_fs = 0, acc_nb = 0;
-    for (int q = tid; q < MH; q += T) {
-        const int packed = sm.home[q];
-        const int si = packed & 0xffff, h = packed >> 16;
-        float4 m = sm.sp[si];
-        const unsigned wm = __float_as_uint(m.w);
-        const int tm = wm >> 31;
-        float fx = 0.f, fy = 0.f, fz = 0.f, pot = 0.f, vir = 0.f;
-        int nbr = 0;
-        unsigned long long nh_hash = 0;
-        for (int dz = -1; dz <= 1; dz++)
-            for (int dy = -1; dy <= 1; dy++)
-                for (int dx = -1; dx <= 1; dx++) {
-                    const int hh = h + dx + hx * (dy + hy * dz);
-                    const int st = sm.start[hh], en = sm.start[hh + 1];
-                    if (st == en) continue;
-                    const unsigned cd = sm.code[hh];
-                    const int cx = (int)(cd & 3) - 1, cy = (int)((cd >> 2) & 3) - 1, cz = (int)((cd >> 4) & 3) - 1;
-                    const float shx = cx == 0 ? 0.f : (cx > 0 ? L : -L);
-                    const float shy = cy == 0 ? 0.f : (cy > 0 ? L : -L);
-                    const float shz = cz == 0 ? 0.f : (cz > 0 ? L : -L);
-                    for (int j = st; j < en; j++) {
-                        const float4 n = sm.sp[j];
-                        const unsigned wn = __float_as_uint(n.w);
-                        if (wn == wm) continue;
-                        const float ddx = __fsub_rn(__fsub_rn(n.x, m.x), shx);
-                        const float ddy = __fsub_rn(__fsub_rn(n.y, m.y), shy);
-                        const float ddz = __fsub_rn(__fsub_rn(n.z, m.z), shz);
-                        const float d2 = dist2_rn(ddx, ddy, ddz);
-                        const int pt = tm + (int)(wn >> 31);
-                        const float c2 = pt == 0 ? c2bb : (pt == 1 ? c2bs : c2ss);
-                        if (d2 < c2) {
-                            const float sg = pt == 0 ? sgbb : (pt == 1 ? sgbs : sgss);
-                            PairOut o = wca_modified_pair(sg, d2, ddx, ddy, ddz);
-                            fx += o.fx;
-                            fy += o.fy;
-                            fz += o.fz;
-                            if (OBS) { pot += o.pot; vir += o.vir; }
-                            if (CENSUS) {
-                                nbr++;
-                                int gidn = __ldg(a.gid_of + (wn & 0x7fffffffu)) - S.part_base;
-                                nh_hash += (unsigned long long)(gidn + 1) * 0x9E3779B97F4A7C15ull;
-                            }
-                        }
-                    }
-                }
-        if (S.fcap > 0.f) {  // capped forces for the initial relaxation
-            float fmx = fmaxf(fabsf(fx), fmaxf(fabsf(fy), fabsf(fz)));
-            if (fmx > 0.f && isfinite(fmx)) {
-                float gx = fx / fmx, gy = fy / fmx, gz = fz / fmx;
-                float ng = sqrtf(gx * gx + gy * gy + gz * gz);
-                if (fmx * ng > S.fcap) {
-                    float sc = S.fcap / ng;
-                    fx = gx * sc; fy = gy * sc; fz = gz * sc;
-                }
-            } else if (!isfinite(fmx)) {
-                fx = fy = fz = 0.f;
-            }
-        }
-        const int sid = wm & 0x7fffffff;
-        const int gid = __ldg(a.gid_of + sid);
-        const int pid = gid - S.part_base;
-        float lx = __ldcg(a.lo_x + sid), ly = __ldcg(a.lo_y + sid), lz = __ldcg(a.lo_z + sid);
-        double qx = __ldcg(a.dsp_x + sid), qy = __ldcg(a.dsp_y + sid), qz = __ldcg(a.dsp_z + sid);
-        if (OBS) {
-            if (tm == 0) acc_pb += pot; else acc_ps += pot;
-            acc_v += vir;
-            double r2 = qx * qx + qy * qy + qz * qz;
-            if (tm == 0) {
-                acc_mb += r2;
-                double r = sqrt(r2), qr = (double)a.qmax * r;
-                acc_fs += (r > 0.0) ? sin(qr) / qr : 1.0;
-            } else {
-                acc_ms += r2;
-            }
-            a.snap[gid] = make_float4(m.x, m.y, m.z, __int_as_float(tm));
-        }
-        if (CENSUS) {
-            acc_nb += nbr;
-            a.nbr_count[gid] = nbr;
-            a.nbr_hash[gid] = nh_hash;
-        }
-        if (!a.do_update) continue;
-        if (ni == 0) {  // origin of the unwrapped positions (main.cu:497-506)
-            qx = qy = qz = 0.0;
-            a.x0[3 * (size_t)gid] = (double)m.x + (double)lx;
-            a.x0[3 * (size_t)gid + 1] = (double)m.y + (double)ly;
-            a.x0[3 * (size_t)gid + 2] = (double)m.z + (double)lz;
-        }
-        float3 xi;
-        if (RNG == kRngPhilox) {
-            xi = gauss3(S.seed, (uint32_t)pid, (uint64_t)ni, a.rng_stream);
-        } else if (RNG == kRngCurand) {
-            curandState *stp = (curandState *)a.curand_states + gid;
-            curandState st = *stp;
-            xi.x = curand_normal(&st);
-            xi.y = curand_normal(&st);
-            xi.z = curand_normal(&st);
-            *stp = st;
-        } else {
-            xi = make_float3(a.noise[3 * (size_t)gid], a.noise[3 * (size_t)gid + 1], a.noise[3 * (size_t)gid + 2]);
-        }
-        const float mob = S.mob[tm], amp = sm.amp[tm], dt = S.dt;
-        // displacement: F*mob*dt + amp*xi (update_ermak.cu:122-134), rounded as written
-        const float ex = __fadd_rn(__fmul_rn(__fmul_rn(fx, mob), dt), __fmul_rn(amp, xi.x));
-        const float ey = __fadd_rn(__fmul_rn(__fmul_rn(fy, mob), dt), __fmul_rn(amp, xi.y));
-        const float ez = __fadd_rn(__fmul_rn(__fmul_rn(fz, mob), dt), __fmul_rn(amp, xi.z));
-        float x = m.x, y = m.y, z = m.z;
-        advance_wrap(x, lx, ex, L, S.Linv);
-        advance_wrap(y, ly, ey, L, S.Linv);
-        advance_wrap(z, lz, ez, L, S.Linv);
-        qx += (double)ex;
-        qy += (double)ey;
-        qz += (double)ez;
-        __stcg(a.lo_x + sid, lx);
-        __stcg(a.lo_y + sid, ly);
-        __stcg(a.lo_z + sid, lz);
-        __stcg(a.dsp_x + sid, qx);
-        __stcg(a.dsp_y + sid, qy);
-        __stcg(a.dsp_z + sid, qz);
-        int ix = (int)__fmul_rn(x, S.cinv), iy = (int)__fmul_rn(y, S.cinv), iz = (int)__fmul_rn(z, S.cinv);
-        if (!(isfinite(x) && isfinite(y) && isfinite(z))) {
-            set_status(a.status, kStatNumeric);
-            ix = iy = iz = 0;
-        }
-        ix = min(max(ix, 0), nc - 1);
-        iy = min(max(iy, 0), nc - 1);
-        iz = min(max(iz, 0), nc - 1);
-        const int cell = S.cell_base + ix + nc * (iy + nc * iz);
-        const int slot = atomicAdd(a.cnt_out + cell, 1);
-        if (slot < a.cap)
-            __stcg(a.pos_out + (size_t)cell * a.cap + slot, make_float4(x, y, z, m.w));
-        else
-            set_status(a.status, kStatCellOverflow);
-    }
-    if (OBS || CENSUS) {
-        double *o = a.obs + (size_t)br.x * kObsCount;
-        double v;
-        if (OBS) {
-            v = block_sum(acc_pb, sm.red); if (tid == 0 && v != 0.0) atomicAdd(o + kObsPotBig, v);
-            v = block_sum(acc_ps, sm.red); if (tid == 0 && v != 0.0) atomicAdd(o + kObsPotSml, v);
-            v = block_sum(acc_v, sm.red); if (tid == 0 && v != 0.0) atomicAdd(o + kObsVir, v);
-            v = block_sum(acc_mb, sm.red); if (tid == 0 && v != 0.0) atomicAdd(o + kObsMsdBig, v);
-            v = block_sum(acc_ms, sm.red); if (tid == 0 && v != 0.0) atomicAdd(o + kObsMsdSml, v);
-            v = block_sum(acc_fs, sm.red); if (tid == 0 && v != 0.0) atomicAdd(o + kObsFsBig, v);
-        }
-        if (CENSUS) { v = block_sum(acc_nb, sm.red); if (tid == 0 && v != 0.0) atomicAdd(o + kObsNbr, v); }
-    }
-    // 4. clear the third count buffer for this brick's own cells
-    if (a.do_update)
-        for (int h = tid; h < nh; h += T) {
-            int lx = h % hx, ly = (h / hx) % hy, lz = h / (hx * hy);
-            if (lx >= 1 && lx <= wx && ly >= 1 && ly <= wy && lz >= 1 && lz <= wz) a.cnt_clr[sm.gc[h]] = 0;
-        }
-}
-
-template <int RNG, bool OBS, bool CENSUS>
-__global__ void __launch_bounds__(256) k_step(StepArgs a, const long long *ni_base, int ni_off) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const long long ni = *ni_base + ni_off;
-    process_brick<RNG, OBS, CENSUS>(a, blockIdx.x, ni, smem);
-}
+}  // namespace bd
+#include "step.cuh"
+namespace bd {
 
 __global__ void k_advance_counter(long long *ni_base, int k) { *ni_base += k; }
 

@@ -47,6 +47,10 @@ def parse():
     ap.add_argument("--replicas", type=int, default=64)
     ap.add_argument("--md-steps", type=int, default=960)
     ap.add_argument("--no-extras", action="store_true", help="skip plain/e2e/reference-CUDA/CPU legs")
+    ap.add_argument("--brick", type=int, nargs=3, default=None, help="cells per brick (default: engine's)")
+    ap.add_argument("--threads", type=int, default=0, help="CTA size (default: engine's)")
+    ap.add_argument("--relax-steps", type=int, default=2000,
+                    help="capped-force relaxation steps; 0 starts from a jittered lattice instead")
     return ap.parse_args()
 
 
@@ -91,17 +95,20 @@ def workload_systems(name, replicas, rank):
     return out, desc
 
 
-def relaxed_positions(systems, seed):
-    """Uniform random positions relaxed by 2000 capped-force steps on the GPU
-    (Philox stream 1), all replicas at once."""
+def relaxed_positions(systems, seed, steps=2000):
+    """Uniform random positions relaxed by `steps` capped-force steps on the
+    GPU (Philox stream 1), all replicas at once; steps=0: jittered lattice."""
     from bd_aging_b200 import configs as CF
     from bd_aging_b200 import lib as B
     import dataclasses
+    if steps <= 0:
+        return np.concatenate([CF.lattice_config(s.n_big, s.n_sml, s.side, seed + k, jitter=0.05)
+                               for k, s in enumerate(systems)])
     pos = np.concatenate([CF.uniform_config(s.n_big, s.n_sml, s.side, seed + k) for k, s in enumerate(systems)])
     relax = [dataclasses.replace(s, dt=1e-4, protocol="const", T0=1.0, force_cap=100.0) for s in systems]
     e = B.Engine(relax, rng_stream=1)
     e.set_positions(pos)
-    e.run(2000)
+    e.run(steps)
     p, _ = e.get_positions()
     e.close()
     return p
@@ -271,10 +278,10 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     systems, desc = workload_systems(args.workload, args.replicas, rank)
-    pos = relaxed_positions(systems, 777 + rank)
+    pos = relaxed_positions(systems, 777 + rank, args.relax_steps)
     P = sum(s.n for s in systems)
     S = args.md_steps
-    eng = B.Engine(systems, graph_steps=96)
+    eng = B.Engine(systems, graph_steps=96, brick=args.brick, threads=args.threads)
     eng.set_positions(pos)
     info = eng.info()
     for _ in range(args.warmup):
@@ -313,7 +320,7 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_extras:
         # plain single-replica engine, same system
         s1 = systems[0]
-        e1 = B.Engine([s1], graph_steps=96)
+        e1 = B.Engine([s1], graph_steps=96, brick=args.brick, threads=args.threads)
         e1.set_positions(pos[: s1.n])
         e1.run(S)
         k1 = max(3, args.steps)
