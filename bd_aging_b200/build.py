@@ -20,7 +20,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libbd_aging_b200.so")
 CLI = os.path.join(HERE, "bd_aging_self")
 
-SOURCES = ["mirror.cu", "engine.cu", "cv3d.cu"]
+SOURCES = ["mirror.cu", "engine.cu", "cv3d.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
               "-I" + os.path.join(ROOT, "include"), "--expt-relaxed-constexpr"] + ARCH

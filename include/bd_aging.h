@@ -163,6 +163,17 @@ int bd_gder_normalize(const double *counts, int nbins, float bin_size, float sid
 int bd_fself_isotropic(const float *rr_raw, const float *rr0, int ngrain, float *fself_host, int sample_number,
                        float qmax, void *stream);
 
+/* No counterpart in the reference.  Same result as bd_fself_isotropic for
+ * callers that cannot allocate device memory when they sample F_s (inside a
+ * stream capture in global capture mode, real-time loops, hosts whose device
+ * memory is reserved by another allocator): its scratch is a fixed 32 KB
+ * device array per GPU, held until process exit, so it calls no cudaMalloc.
+ * Limit: ngrain <= 1,048,576, larger calls return BD_ERR_ARG.  The first call
+ * on a device looks up the scratch address; make it before any stream
+ * capture.  Calls that overlap on the GPU share the scratch and race. */
+int bd_fself_isotropic_noalloc(const float *rr_raw, const float *rr0, int ngrain, float *fself_host,
+                               int sample_number, float qmax, void *stream);
+
 /* Mean squared displacement of main.cu:776-792 for one species: returns
  * (1/N) sum |rr_raw - rr0|^2 in *msd_host.  Stream-synchronous. */
 int bd_msd(const float *rr_raw, const float *rr0, int ngrain, float *msd_host, void *stream);
