@@ -109,7 +109,7 @@ struct bd_engine {
     float qmax = 6.2831853f;
     bool loaded = false;
     int graph_steps = 96;
-    cudaGraphExec_t gexec = nullptr;
+    cudaGraphExec_t gexec[3] = {nullptr, nullptr, nullptr};  // one per rotation phase e->cur
     int autotune = 0;
     bool tuned = false;
 };
@@ -140,6 +140,7 @@ StepArgs make_args(bd_engine *e, int buf, int do_update) {
     a.lo_x = e->lo[0]; a.lo_y = e->lo[1]; a.lo_z = e->lo[2];
     a.dsp_x = e->dsp[0]; a.dsp_y = e->dsp[1]; a.dsp_z = e->dsp[2];
     a.gid_of = e->gid_of;
+    a.np = (int)e->P;
     a.x0 = e->x0;
     a.snap = e->snap;
     a.obs = e->obs;
@@ -215,7 +216,9 @@ int plain_step(bd_engine *e) {
 }
 
 int build_graph(bd_engine *e) {
-    if (e->gexec) return BD_OK;
+    // The recorded launches bake in the buffer rotation of e->cur, so each
+    // rotation phase gets its own graph.
+    if (e->gexec[e->cur]) return BD_OK;
     cudaGraph_t g;
     BD_CUDA_TRY(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
     int rc = BD_OK;
@@ -227,13 +230,14 @@ int build_graph(bd_engine *e) {
     cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
     if (rc) return rc;
     BD_CUDA_TRY(ce);
-    BD_CUDA_TRY(cudaGraphInstantiate(&e->gexec, g, 0));
+    BD_CUDA_TRY(cudaGraphInstantiate(&e->gexec[e->cur], g, 0));
     cudaGraphDestroy(g);
     return BD_OK;
 }
 
 void free_engine(bd_engine *e) {
-    if (e->gexec) cudaGraphExecDestroy(e->gexec);
+    for (int k = 0; k < 3; k++)
+        if (e->gexec[k]) cudaGraphExecDestroy(e->gexec[k]);
     void *ptrs[] = {e->d_sys, e->d_bricks, e->cnt[0], e->cnt[1], e->cnt[2], e->pos[0], e->pos[1], e->pos[2],
                     e->lo[0], e->lo[1], e->lo[2], e->dsp[0], e->dsp[1], e->dsp[2], e->gid_of, e->rep_of_sid,
                     e->rep_of_gid, e->x0, e->obs, e->snap, e->nbr_count, e->nbr_hash, e->cr, e->noise,
@@ -293,7 +297,7 @@ int setup_geometry(bd_engine *e) {
     e->P = part_base;
     e->nbricks = (int)e->bricks_h.size();
     const int nh = (e->bx + 2) * (e->by + 2) * (e->bz + 2);
-    e->smax = std::min(65535, std::max(256, (7 * nh) / 2));
+    e->smax = std::min(65534, std::max(256, (7 * nh) / 2)) & ~1;  // even: 8-byte aligned views
     e->smem = brick_smem_bytes(nh, e->smax, e->threads);
     e->smem_census = e->smem;
     if (e->smem_census > 227 * 1024) return BD_ERR_ARG;
@@ -327,6 +331,7 @@ int bd_engine_create(const bd_system_desc *systems, int nsys, const bd_engine_op
     e->rng = opts.rng;
     if (e->rng < 0 || e->rng > 2) { delete e; return BD_ERR_ARG; }
     e->cap = opts.cell_capacity > 0 ? opts.cell_capacity : 16;
+    if (e->cap > kQueue / 3) { delete e; return BD_ERR_ARG; }  // a row of 3 cells must fit one queue
     if (opts.brick[0] > 0 && opts.brick[1] > 0 && opts.brick[2] > 0) {
         e->bx = opts.brick[0]; e->by = opts.brick[1]; e->bz = opts.brick[2];
     }
@@ -485,7 +490,7 @@ int bd_engine_set_positions(bd_engine *e, const float *pos) {
     cudaStreamSynchronize(e->stream);
     cudaFree(d_staged);
     if (le != cudaSuccess) return BD_ERR_CUDA;
-    if (e->gexec) { cudaGraphExecDestroy(e->gexec); e->gexec = nullptr; }
+
     e->loaded = true;
     return engine_status(e);
 }
@@ -498,7 +503,7 @@ int bd_engine_run(bd_engine *e, long long nsteps) {
         if (nsteps >= e->graph_steps && e->rng != BD_RNG_NOISE) {
             int rc = build_graph(e);
             if (rc) return rc;
-            BD_CUDA_TRY(cudaGraphLaunch(e->gexec, e->stream));
+            BD_CUDA_TRY(cudaGraphLaunch(e->gexec[e->cur], e->stream));
             e->ni += e->graph_steps;  // cur unchanged: graph_steps is a multiple of 3
             nsteps -= e->graph_steps;
         } else {
@@ -553,7 +558,7 @@ int bd_engine_get_positions(bd_engine *e, float *pos_host, float *raw_host) {
         if (cudaMalloc(&e->out_pos, sizeof(float) * 3 * P) != cudaSuccess) return BD_ERR_NOMEM;
         if (cudaMalloc(&e->out_raw, sizeof(float) * 3 * P) != cudaSuccess) return BD_ERR_NOMEM;
     }
-    k_export<<<div_up(e->C, 128), 128, 0, e->stream>>>(e->cnt[e->cur], e->pos[e->cur], (int)e->C, e->cap, e->gid_of,
+    k_export<<<div_up(e->C, 128), 128, 0, e->stream>>>(e->cnt[e->cur], e->pos[e->cur], (int)e->C, e->cap, (int)e->P, e->gid_of,
                                                        e->x0, e->dsp[0], e->dsp[1], e->dsp[2], e->out_pos,
                                                        e->out_raw, e->snap);
     BD_LAUNCH_CHECK();
@@ -565,7 +570,7 @@ int bd_engine_get_positions(bd_engine *e, float *pos_host, float *raw_host) {
 int bd_engine_gder(bd_engine *e, int nbins, float range, unsigned long long *counts_host) {
     if (!e || !counts_host || nbins < 1 || nbins > 4096 || !(range > 0)) return BD_ERR_ARG;
     if (!e->loaded) return BD_ERR_STATE;
-    k_export<<<div_up(e->C, 128), 128, 0, e->stream>>>(e->cnt[e->cur], e->pos[e->cur], (int)e->C, e->cap, e->gid_of,
+    k_export<<<div_up(e->C, 128), 128, 0, e->stream>>>(e->cnt[e->cur], e->pos[e->cur], (int)e->C, e->cap, (int)e->P, e->gid_of,
                                                        e->x0, e->dsp[0], e->dsp[1], e->dsp[2], nullptr, nullptr,
                                                        e->snap);
     BD_LAUNCH_CHECK();

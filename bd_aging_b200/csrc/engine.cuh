@@ -70,6 +70,7 @@ struct StepArgs {
     float *lo_x, *lo_y, *lo_z;
     double *dsp_x, *dsp_y, *dsp_z;
     const int *gid_of;
+    int np;              // particles in the batch (bound for storage ids)
     double *x0;          // [3P] origin of the unwrapped positions, by gid
     float4 *snap;        // [P] positions by gid, written by observation passes
     double *obs;         // [R][kObsCount]

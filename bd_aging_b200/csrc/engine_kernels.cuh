@@ -136,7 +136,7 @@ __global__ void k_load(const float4 *__restrict__ staged, int P, const int *__re
 }
 // Export current positions by global index: wrapped (hi) and unwrapped
 // (origin + displacement) float3.
-__global__ void k_export(const int *__restrict__ cnt, const float4 *__restrict__ pos, int C, int cap,
+__global__ void k_export(const int *__restrict__ cnt, const float4 *__restrict__ pos, int C, int cap, int P,
                          const int *__restrict__ gid_of, const double *__restrict__ x0,
                          const double *__restrict__ dx, const double *__restrict__ dy, const double *__restrict__ dz,
                          float *out_pos, float *out_raw, float4 *snap) {
@@ -146,7 +146,9 @@ __global__ void k_export(const int *__restrict__ cnt, const float4 *__restrict__
     for (int s = 0; s < k; s++) {
         float4 v = pos[(size_t)c * cap + s];
         unsigned w = __float_as_uint(v.w);
-        int sid = w & 0x7fffffff, gid = gid_of[sid];
+        int sid = w & 0x7fffffff;
+        if (sid >= P) continue;  // never true for consistent buffers
+        int gid = gid_of[sid];
         if (out_pos) { out_pos[3 * (size_t)gid] = v.x; out_pos[3 * (size_t)gid + 1] = v.y; out_pos[3 * (size_t)gid + 2] = v.z; }
         if (out_raw) {
             out_raw[3 * (size_t)gid] = (float)(x0[3 * (size_t)gid] + dx[sid]);

@@ -5,12 +5,14 @@
 // force clears + get_forces_*_dev x4) becomes one pass over the brick:
 //   1. stage the brick's cells plus a one-cell halo into shared memory: cell
 //      counts -> block scan -> one independent load per staged particle ->
-//      each cell sorted by storage id (so every force sum has a fixed order);
+//      scatter to its rank within the cell by storage id (every force sum then
+//      has a fixed order, independent of brick shape and batching);
 //   2. every home particle sweeps the 9 rows of 3 contiguous neighbour cells
-//      with the per-species-pair cut distances (bb, bs, ss) in one pass; the
-//      cut-off test rounds like the reference (get_forces.cu:383-396) and
-//      interacting partners are queued, then evaluated after the sweep so the
-//      pair arithmetic runs only for lanes that need it;
+//      two candidates at a time with packed f32x2 arithmetic; the cut-off
+//      test rounds like the reference (get_forces.cu:383-396) and reads the
+//      squared cut distance from a per-home-species view of the staged
+//      particles (bb, bs, ss without a per-candidate select); interacting
+//      partners are queued and evaluated after the sweep;
 //   3. Ermak-McCammon update of that particle with counter-based Gaussians,
 //      compensated FP32 position + FP64 displacement;
 //   4. the new position is binned into the next count/position buffer and
@@ -20,17 +22,48 @@
 
 namespace bd {
 
-constexpr int kQueue = 32;  // queued interacting partners per thread before a flush
+constexpr int kQueue = 48;            // queue length per thread; >= one row (3 cells x 16 slots)
+constexpr unsigned kNoShift = 0x15u;  // shift code of a halo cell that did not wrap
+
+typedef unsigned long long f2;  // two floats in one 64-bit register (lo, hi)
+__device__ __forceinline__ f2 f2_bcast(float v) {
+    f2 r;
+    asm("mov.b64 %0, {%1, %1};" : "=l"(r) : "f"(v));
+    return r;
+}
+__device__ __forceinline__ void f2_split(f2 v, float &lo, float &hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2 f2_add(f2 a, f2 b) {
+    f2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2 f2_sub(f2 a, f2 b) {
+    f2 d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2 f2_mul(f2 a, f2 b) {
+    f2 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
 
 struct BrickSmem {
-    int *start;            // [nh+1] staged-particle prefix over halo cells
-    int *hstart;           // [nh+1] home-particle prefix over halo cells
-    int *gc;               // [nh]   global cell index
-    unsigned char *code;   // [nh]   periodic shift code (2 bits per axis)
-    float4 *sp;            // [smax] staged particles: x, y, z, w = species | code << 1
-    int *ssid;             // [smax] storage id of each staged particle
-    int *home;             // [smax] staged index | halo cell << 16, per home particle
-    unsigned short *queue; // [kQueue][threads] interacting partners (staged index)
+    int *start;             // [nh+1] staged-particle prefix over halo cells
+    int *hstart;            // [nh+1] home-particle prefix over halo cells
+    int *gc;                // [nh]   global cell index
+    unsigned char *code;    // [nh]   periodic shift code (2 bits per axis)
+    float *xs, *ys, *zs;    // [smax+2] staged positions, sorted by storage id in each cell
+    float *c2v;             // [2][smax+2] squared cut distance towards each staged
+                            //   particle, seen from a big / a small home particle
+    unsigned char *tc;      // [smax] species | shift code << 1
+    int *ssid;              // [smax] storage id
+    int *home;              // [smax] staged index | halo cell << 16, per home particle
+    float4 *raw;            // [smax] unsorted staging   (shares memory with queue)
+    unsigned short *queue;  // [kQueue][threads]          (shares memory with raw)
+    unsigned short *hslot;  // [smax] halo cell of each unsorted slot
     double *red;
     int *tmp;
     float *amp;
@@ -46,20 +79,30 @@ __host__ __device__ inline size_t brick_smem_layout(int nh, int smax, int thread
         off += bytes;
         return q;
     };
-    unsigned char *p_sp = take((size_t)smax * 16, 16);
+    const size_t ns = (size_t)smax + 2;
+    size_t uni = (size_t)smax * 16;
+    if ((size_t)kQueue * threads * 2 > uni) uni = (size_t)kQueue * threads * 2;
+    unsigned char *p_uni = take(uni, 16);
+    unsigned char *p_xs = take(ns * 4, 16);
+    unsigned char *p_ys = take(ns * 4, 16);
+    unsigned char *p_zs = take(ns * 4, 16);
+    unsigned char *p_c2 = take(2 * ns * 4, 16);
     unsigned char *p_start = take((size_t)(nh + 1) * 4, 4);
     unsigned char *p_hstart = take((size_t)(nh + 1) * 4, 4);
     unsigned char *p_gc = take((size_t)nh * 4, 4);
     unsigned char *p_ssid = take((size_t)smax * 4, 4);
     unsigned char *p_home = take((size_t)smax * 4, 4);
-    unsigned char *p_queue = take((size_t)kQueue * threads * 2, 4);
+    unsigned char *p_hslot = take((size_t)smax * 2, 4);
+    unsigned char *p_tc = take((size_t)smax, 4);
     unsigned char *p_code = take((size_t)nh, 4);
     unsigned char *p_red = take(32 * 8, 8);
     unsigned char *p_tmp = take(64 * 4, 4);
     unsigned char *p_amp = take(16, 4);
     if (s) {
-        s->sp = (float4 *)p_sp; s->start = (int *)p_start; s->hstart = (int *)p_hstart; s->gc = (int *)p_gc;
-        s->ssid = (int *)p_ssid; s->home = (int *)p_home; s->queue = (unsigned short *)p_queue; s->code = p_code;
+        s->raw = (float4 *)p_uni; s->queue = (unsigned short *)p_uni;
+        s->xs = (float *)p_xs; s->ys = (float *)p_ys; s->zs = (float *)p_zs; s->c2v = (float *)p_c2;
+        s->start = (int *)p_start; s->hstart = (int *)p_hstart; s->gc = (int *)p_gc; s->ssid = (int *)p_ssid;
+        s->home = (int *)p_home; s->hslot = (unsigned short *)p_hslot; s->tc = p_tc; s->code = p_code;
         s->red = (double *)p_red; s->tmp = (int *)p_tmp; s->amp = (float *)p_amp;
     }
     return off;
@@ -69,8 +112,8 @@ __host__ __device__ inline size_t brick_smem_bytes(int nh, int smax, int threads
 }
 
 // periodic shift of a staged particle along one axis: code bits -> -L, 0, +L
-__device__ __forceinline__ float axis_shift(unsigned w, int axis, float L) {
-    const int c = (int)((w >> (1 + 2 * axis)) & 3u) - 1;
+__device__ __forceinline__ float axis_shift(unsigned tc, int axis, float L) {
+    const int c = (int)((tc >> (1 + 2 * axis)) & 3u) - 1;
     return __int2float_rn(c) * L;  // exact: c in {-1, 0, 1}
 }
 
@@ -80,23 +123,20 @@ struct PairSums {
     unsigned long long hsh = 0;
 };
 
-// Evaluate the queued partners of home particle m (staged index list in
-// queue column `tid`), in queue order.
+// Evaluate the queued partners of one home particle in queue order.
 template <bool OBS, bool CENSUS>
-__device__ __forceinline__ void flush_queue(const BrickSmem &sm, const StepArgs &a, int nq, float4 m, int tm,
-                                            bool wrapx, bool wrapy, bool wrapz, float L, float sgbb, float sgbs,
-                                            float sgss, int part_base, PairSums &ps) {
+__device__ __forceinline__ void flush_queue(const BrickSmem &sm, const StepArgs &a, int nq, float mx, float my,
+                                            float mz, int tm, float L, float sgbb, float sgbs, float sgss,
+                                            int part_base, PairSums &ps) {
     const int T = blockDim.x, tid = threadIdx.x;
     for (int e = 0; e < nq; e++) {
         const int j = sm.queue[e * T + tid];
-        const float4 n = sm.sp[j];
-        const unsigned wn = __float_as_uint(n.w);
-        float dx = __fsub_rn(n.x, m.x), dy = __fsub_rn(n.y, m.y), dz = __fsub_rn(n.z, m.z);
-        if (wrapx) dx = __fsub_rn(dx, axis_shift(wn, 0, L));
-        if (wrapy) dy = __fsub_rn(dy, axis_shift(wn, 1, L));
-        if (wrapz) dz = __fsub_rn(dz, axis_shift(wn, 2, L));
+        const unsigned tcj = sm.tc[j];
+        const float dx = __fsub_rn(__fsub_rn(sm.xs[j], mx), axis_shift(tcj, 0, L));
+        const float dy = __fsub_rn(__fsub_rn(sm.ys[j], my), axis_shift(tcj, 1, L));
+        const float dz = __fsub_rn(__fsub_rn(sm.zs[j], mz), axis_shift(tcj, 2, L));
         const float d2 = dist2_rn(dx, dy, dz);
-        const int pt = tm + (int)(wn & 1u);
+        const int pt = tm + (int)(tcj & 1u);
         const float sg = pt == 0 ? sgbb : (pt == 1 ? sgbs : sgss);
         // WCA-modified pair (potentials.cu:137-147) in terms of 1/r
         const float di = rsqrtf(d2);
@@ -114,9 +154,46 @@ __device__ __forceinline__ void flush_queue(const BrickSmem &sm, const StepArgs 
         }
         if (CENSUS) {
             ps.nbr++;
-            const int gidn = __ldg(a.gid_of + sm.ssid[j]) - part_base;
+            const int sj = sm.ssid[j];
+            const int gidn = ((unsigned)sj < (unsigned)a.np ? __ldg(a.gid_of + sj) : part_base) - part_base;
             ps.hsh += (unsigned long long)(gidn + 1) * 0x9E3779B97F4A7C15ull;
         }
+    }
+}
+
+// One row of candidates [j0, j1) against home particle si.  MID: the row
+// holding the home particle itself (excluded by index, like the reference's
+// nn == mm test).  Rows that cross the periodic box take the scalar path with
+// the per-candidate shift; all others are swept two candidates at a time.
+template <bool MID>
+__device__ __forceinline__ void sweep_row(const BrickSmem &sm, const float *view, int j0, int j1, int si, bool wrap,
+                                          float mx, float my, float mz, f2 mxx, f2 myy, f2 mzz, float L, int &nq) {
+    const int T = blockDim.x, tid = threadIdx.x;
+    unsigned short *q = sm.queue + tid;
+    if (wrap) {
+        for (int j = j0; j < j1; j++) {
+            const unsigned tcj = sm.tc[j];
+            const float dx = __fsub_rn(__fsub_rn(sm.xs[j], mx), axis_shift(tcj, 0, L));
+            const float dy = __fsub_rn(__fsub_rn(sm.ys[j], my), axis_shift(tcj, 1, L));
+            const float dz = __fsub_rn(__fsub_rn(sm.zs[j], mz), axis_shift(tcj, 2, L));
+            const bool hit = dist2_rn(dx, dy, dz) < view[j] && (!MID || j != si);
+            if (hit) q[(nq++) * T] = (unsigned short)j;
+        }
+        return;
+    }
+#pragma unroll 2
+    for (int j = j0 & ~1; j < j1; j += 2) {
+        const f2 dx = f2_sub(*reinterpret_cast<const f2 *>(sm.xs + j), mxx);
+        const f2 dy = f2_sub(*reinterpret_cast<const f2 *>(sm.ys + j), myy);
+        const f2 dz = f2_sub(*reinterpret_cast<const f2 *>(sm.zs + j), mzz);
+        const f2 d2 = f2_add(f2_add(f2_mul(dx, dx), f2_mul(dy, dy)), f2_mul(dz, dz));
+        float d2a, d2b, ca, cb;
+        f2_split(d2, d2a, d2b);
+        f2_split(*reinterpret_cast<const f2 *>(view + j), ca, cb);
+        const bool ha = d2a < ca && j >= j0 && (!MID || j != si);
+        const bool hb = d2b < cb && j + 1 < j1 && (!MID || j + 1 != si);
+        if (ha) q[(nq++) * T] = (unsigned short)j;
+        if (hb) q[(nq++) * T] = (unsigned short)(j + 1);
     }
 }
 
@@ -128,10 +205,10 @@ __device__ void process_brick(const StepArgs &a, int bidx, long long ni, unsigne
     const int ox = br.y, oy = br.z, oz = br.w;
     const int wx = min(a.bx, nc - ox), wy = min(a.by, nc - oy), wz = min(a.bz, nc - oz);
     const int hx = wx + 2, hy = wy + 2, hz = wz + 2, nh = hx * hy * hz;
-    const bool wrapx = ox == 0 || ox + wx == nc, wrapy = oy == 0 || oy + wy == nc, wrapz = oz == 0 || oz + wz == nc;
     BrickSmem sm;
     brick_smem_layout((a.bx + 2) * (a.by + 2) * (a.bz + 2), a.smax, blockDim.x, &sm, smem_raw);
     const int tid = threadIdx.x, T = blockDim.x;
+    const int vstride = a.smax + 2;
     const float L = S.L, Linv = S.Linv, cinv = S.cinv;
     const int cell_base = S.cell_base, part_base = S.part_base;
     const float c2bb = S.cut2[0], c2bs = S.cut2[1], c2ss = S.cut2[2];
@@ -153,6 +230,7 @@ __device__ void process_brick(const StepArgs &a, int bidx, long long ni, unsigne
         const int gc = cell_base + gx + nc * (gy + nc * gz);
         int c = __ldcg(a.cnt_in + gc);
         if (c > a.cap) { set_status(a.status, kStatCellOverflow); c = a.cap; }
+        if (c < 0) { set_status(a.status, kStatArg); c = 0; }  // never true for consistent buffers
         const bool home = lx >= 1 && lx <= wx && ly >= 1 && ly <= wy && lz >= 1 && lz <= wz;
         sm.gc[h] = gc;
         sm.start[h] = c;
@@ -166,76 +244,70 @@ __device__ void process_brick(const StepArgs &a, int bidx, long long ni, unsigne
         if (tid == 0) set_status(a.status, kStatCellOverflow);
         return;
     }
-    // 2. one independent load per staged particle
+    // 2a. one independent load per staged particle (unsorted)
     for (int t = tid; t < M; t += T) {
         int lo = 0, hi = nh - 1;  // last halo cell with start <= t
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
             if (sm.start[mid] <= t) lo = mid; else hi = mid - 1;
         }
-        const float4 v = __ldcg(a.pos_in + (size_t)sm.gc[lo] * a.cap + (t - sm.start[lo]));
-        const unsigned w = __float_as_uint(v.w);
-        sm.sp[t] = make_float4(v.x, v.y, v.z, __uint_as_float((w >> 31) | ((unsigned)sm.code[lo] << 1)));
-        sm.ssid[t] = (int)(w & 0x7fffffffu);
+        sm.raw[t] = __ldcg(a.pos_in + (size_t)sm.gc[lo] * a.cap + (t - sm.start[lo]));
+        sm.hslot[t] = (unsigned short)lo;
+    }
+    if (tid < 2) {  // padding read by the paired sweep past the last staged particle
+        sm.xs[M + tid] = 1e30f; sm.ys[M + tid] = 1e30f; sm.zs[M + tid] = 1e30f;
+        sm.c2v[M + tid] = 0.f; sm.c2v[vstride + M + tid] = 0.f;
     }
     __syncthreads();
-    // 3. sort each cell by storage id; list the home particles
-    for (int h = tid; h < nh; h += T) {
+    // 2b. scatter to the rank within the cell by storage id; list home particles
+    for (int t = tid; t < M; t += T) {
+        const int h = sm.hslot[t];
         const int st = sm.start[h], c = sm.start[h + 1] - st;
-        for (int k = 1; k < c; k++) {
-            const int key = sm.ssid[st + k];
-            const float4 v = sm.sp[st + k];
-            int j = st + k - 1;
-            while (j >= st && sm.ssid[j] > key) { sm.ssid[j + 1] = sm.ssid[j]; sm.sp[j + 1] = sm.sp[j]; j--; }
-            sm.ssid[j + 1] = key;
-            sm.sp[j + 1] = v;
-        }
+        const float4 v = sm.raw[t];
+        const unsigned w = __float_as_uint(v.w), key = w & 0x7fffffffu;
+        int rank = 0;
+        for (int k = 0; k < c; k++) rank += (__float_as_uint(sm.raw[st + k].w) & 0x7fffffffu) < key;
+        const int d = st + rank;
+        const unsigned tn = w >> 31;
+        sm.xs[d] = v.x;
+        sm.ys[d] = v.y;
+        sm.zs[d] = v.z;
+        sm.c2v[d] = tn ? c2bs : c2bb;
+        sm.c2v[vstride + d] = tn ? c2ss : c2bs;
+        sm.tc[d] = (unsigned char)(tn | ((unsigned)sm.code[h] << 1));
+        sm.ssid[d] = (int)key;
         const int hs = sm.hstart[h];
-        if (sm.hstart[h + 1] > hs)
-            for (int k = 0; k < c; k++) sm.home[hs + k] = (st + k) | (h << 16);
+        if (sm.hstart[h + 1] > hs) sm.home[hs + rank] = d | (h << 16);
     }
     __syncthreads();
 
-    // 4. forces and update, one thread per home particle
+    // 3. forces and update, one thread per home particle
     double acc_pb = 0, acc_ps = 0, acc_v = 0, acc_mb = 0, acc_ms = 0, acc_fs = 0, acc_nb = 0;
     for (int q = tid; q < MH; q += T) {
         const int packed = sm.home[q];
         const int si = packed & 0xffff, h = packed >> 16;
-        const float4 m = sm.sp[si];
-        const int tm = (int)(__float_as_uint(m.w) & 1u);
-        // does this particle's 27-cell neighbourhood cross the periodic box?
-        const int hlx = h % hx, hly = (h / hx) % hy, hlz = h / (hx * hy);
-        const bool px = wrapx && (hlx == 1 || hlx == wx), py = wrapy && (hly == 1 || hly == wy),
-                   pz = wrapz && (hlz == 1 || hlz == wz);
-        // cut distances squared towards a partner of the same / the other species
-        const float c2same = tm == 0 ? c2bb : c2ss;
-        const unsigned tmu = (unsigned)tm;
+        const float mx = sm.xs[si], my = sm.ys[si], mz = sm.zs[si];
+        const int tm = (int)(sm.tc[si] & 1u);
+        const float *view = sm.c2v + tm * vstride;
+        const f2 mxx = f2_bcast(mx), myy = f2_bcast(my), mzz = f2_bcast(mz);
         PairSums ps;
         int nq = 0;
         for (int dz = -1; dz <= 1; dz++)
             for (int dy = -1; dy <= 1; dy++) {
                 const int hr = h - 1 + hx * (dy + hy * dz);  // row of 3 contiguous halo cells
                 const int j0 = sm.start[hr], j1 = sm.start[hr + 3];
-#pragma unroll 2
-                for (int j = j0; j < j1; j++) {
-                    const float4 n = sm.sp[j];
-                    const unsigned wn = __float_as_uint(n.w);
-                    float dx = __fsub_rn(n.x, m.x), dy_ = __fsub_rn(n.y, m.y), dz_ = __fsub_rn(n.z, m.z);
-                    if (px) dx = __fsub_rn(dx, axis_shift(wn, 0, L));
-                    if (py) dy_ = __fsub_rn(dy_, axis_shift(wn, 1, L));
-                    if (pz) dz_ = __fsub_rn(dz_, axis_shift(wn, 2, L));
-                    const float d2 = dist2_rn(dx, dy_, dz_);
-                    const float c2 = ((wn ^ tmu) & 1u) ? c2bs : c2same;
-                    if (d2 < c2 && j != si) {
-                        sm.queue[nq * T + tid] = (unsigned short)j;
-                        if (++nq == kQueue) {
-                            flush_queue<OBS, CENSUS>(sm, a, nq, m, tm, px, py, pz, L, sgbb, sgbs, sgss, part_base, ps);
-                            nq = 0;
-                        }
-                    }
+                if (nq + (j1 - j0) > kQueue) {
+                    flush_queue<OBS, CENSUS>(sm, a, nq, mx, my, mz, tm, L, sgbb, sgbs, sgss, part_base, ps);
+                    nq = 0;
                 }
+                const bool wrap =
+                    sm.code[hr] != kNoShift || sm.code[hr + 1] != kNoShift || sm.code[hr + 2] != kNoShift;
+                if (dy == 0 && dz == 0)
+                    sweep_row<true>(sm, view, j0, j1, si, wrap, mx, my, mz, mxx, myy, mzz, L, nq);
+                else
+                    sweep_row<false>(sm, view, j0, j1, si, wrap, mx, my, mz, mxx, myy, mzz, L, nq);
             }
-        flush_queue<OBS, CENSUS>(sm, a, nq, m, tm, px, py, pz, L, sgbb, sgbs, sgss, part_base, ps);
+        flush_queue<OBS, CENSUS>(sm, a, nq, mx, my, mz, tm, L, sgbb, sgbs, sgss, part_base, ps);
         float fx = ps.fx, fy = ps.fy, fz = ps.fz;
         if (S.fcap > 0.f) {  // capped forces for the initial relaxation
             const float fmx = fmaxf(fabsf(fx), fmaxf(fabsf(fy), fabsf(fz)));
@@ -251,6 +323,10 @@ __device__ void process_brick(const StepArgs &a, int bidx, long long ni, unsigne
             }
         }
         const int sid = sm.ssid[si];
+        if ((unsigned)sid >= (unsigned)a.np) {  // never true for consistent buffers
+            set_status(a.status, kStatArg);
+            continue;
+        }
         const int gid = __ldg(a.gid_of + sid);
         const int pid = gid - part_base;
         float lx = __ldcg(a.lo_x + sid), ly = __ldcg(a.lo_y + sid), lz = __ldcg(a.lo_z + sid);
@@ -266,7 +342,7 @@ __device__ void process_brick(const StepArgs &a, int bidx, long long ni, unsigne
             } else {
                 acc_ms += r2;
             }
-            a.snap[gid] = make_float4(m.x, m.y, m.z, __int_as_float(tm));
+            a.snap[gid] = make_float4(mx, my, mz, __int_as_float(tm));
         }
         if (CENSUS) {
             acc_nb += ps.nbr;
@@ -276,9 +352,9 @@ __device__ void process_brick(const StepArgs &a, int bidx, long long ni, unsigne
         if (!a.do_update) continue;
         if (ni == 0) {  // origin of the unwrapped positions (main.cu:497-506)
             qx = qy = qz = 0.0;
-            a.x0[3 * (size_t)gid] = (double)m.x + (double)lx;
-            a.x0[3 * (size_t)gid + 1] = (double)m.y + (double)ly;
-            a.x0[3 * (size_t)gid + 2] = (double)m.z + (double)lz;
+            a.x0[3 * (size_t)gid] = (double)mx + (double)lx;
+            a.x0[3 * (size_t)gid + 1] = (double)my + (double)ly;
+            a.x0[3 * (size_t)gid + 2] = (double)mz + (double)lz;
         }
         float3 xi;
         if (RNG == kRngPhilox) {
@@ -298,7 +374,7 @@ __device__ void process_brick(const StepArgs &a, int bidx, long long ni, unsigne
         const float ex = __fadd_rn(__fmul_rn(__fmul_rn(fx, mob), dt), __fmul_rn(amp, xi.x));
         const float ey = __fadd_rn(__fmul_rn(__fmul_rn(fy, mob), dt), __fmul_rn(amp, xi.y));
         const float ez = __fadd_rn(__fmul_rn(__fmul_rn(fz, mob), dt), __fmul_rn(amp, xi.z));
-        float x = m.x, y = m.y, z = m.z;
+        float x = mx, y = my, z = mz;
         advance_wrap(x, lx, ex, L, Linv);
         advance_wrap(y, ly, ey, L, Linv);
         advance_wrap(z, lz, ez, L, Linv);

@@ -234,7 +234,7 @@ typedef struct bd_system_desc {
 
 typedef struct bd_engine_opts {
     int rng;                   /* BD_RNG_* */
-    int cell_capacity;         /* slots per cell (0 = 16) */
+    int cell_capacity;         /* slots per cell (0 = 16, at most 16) */
     int brick[3];              /* cells per brick (0 = autotune / default) */
     int threads;               /* CTA size (0 = default) */
     int mode;                  /* BD_MODE_* */

@@ -1,0 +1,84 @@
+"""End-to-end drop-in check on the GPU: the reference executable built from
+its sources (oracle/_ref/bd_aging_self.bin) and bd_aging_b200/bd_aging_self
+run on identical inputs (same stdin, same init_config files, same idum, so
+the same cuRAND noise) and their output files are compared."""
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from bd_aging_b200 import configs as CF
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "bd_aging_b200", "bd_aging_self")
+REF = os.path.join(ROOT, "oracle", "_ref", "bd_aging_self.bin")
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not (os.path.exists(CLI) and os.path.exists(REF)),
+                                 reason="needs the CLI and the reference build")]
+
+# run_time 0.0102 with dt 1e-5 gives niter = 1020, five samples (ngap 204)
+DATA = "linear\n1.0  0.5  0.0  0.005  1\n1e-5\nlinear\n0.001  0.0102  5\n16  16\n2\n100  6.0\n6.19\n4321\n"
+# run_time 0.01 gives niter = (int)(0.01/1e-5) = 999 and ngap 199: a sixth
+# sample, which the reference rejects ("counter fuera de rango", exit 1)
+BAD = DATA.replace("0.0102", "0.01")
+
+
+def tree(base, nb, ns, phi, n_configs):
+    (base / "configs").mkdir(parents=True)
+    (base / "simulation" / "results").mkdir(parents=True)
+    side = float(np.float32(CF.side_from_phi(nb, ns, phi)))
+    for k in range(n_configs):
+        CF.write_init_config(str(base / "configs" / ("init_config_%d" % (k + 1))),
+                             CF.lattice_config(nb, ns, side, 40 + k, jitter=0.1), nb, ns, side)
+
+
+def load(path):
+    return np.loadtxt(str(path), ndmin=2)
+
+
+def test_cli_outputs_match_reference_executable(tmp_path):
+    a, b = tmp_path / "ref", tmp_path / "ours"
+    tree(a, 500, 500, 0.45, 2)
+    shutil.copytree(a, b)
+    ra = subprocess.run([REF], input=DATA, cwd=a / "simulation", capture_output=True, text=True, timeout=600)
+    rb = subprocess.run([CLI], input=DATA, cwd=b / "simulation", capture_output=True, text=True, timeout=600)
+    assert ra.returncode == 0, ra.stdout[-2000:] + ra.stderr[-2000:]
+    assert rb.returncode == 0, rb.stdout[-2000:] + rb.stderr[-2000:]
+    assert "TERMINADO" in rb.stdout
+    # bitacora: identical text (geometry, ranges, run lengths)
+    assert (a / "simulation" / "bitacora").read_text() == (b / "simulation" / "bitacora").read_text()
+    res_a, res_b = a / "simulation" / "results", b / "simulation" / "results"
+    assert sorted(os.listdir(res_a)) == sorted(os.listdir(res_b))
+    ea, eb = load(res_a / "energies_averaged.out"), load(res_b / "energies_averaged.out")
+    np.testing.assert_allclose(eb[:, 0], ea[:, 0], atol=1e-6)            # time
+    np.testing.assert_allclose(eb[:, 3], ea[:, 3], atol=1e-6)            # temperature
+    np.testing.assert_allclose(eb[:, 1:3], ea[:, 1:3], rtol=2e-3, atol=2e-5)
+    pa, pb = load(res_a / "pressure.out"), load(res_b / "pressure.out")
+    np.testing.assert_allclose(pb, pa, rtol=2e-3, atol=2e-5)
+    fa, fb = load(res_a / "fself.out"), load(res_b / "fself.out")
+    assert fa[0, 1] == 0.0 and fb[0, 1] == 0.0  # the reference's 1-based F_s index
+    np.testing.assert_allclose(fb, fa, atol=5e-5)
+    ma, mb = load(res_a / "msd_averaged.out"), load(res_b / "msd_averaged.out")
+    np.testing.assert_allclose(mb, ma, rtol=2e-2, atol=3e-6)
+    for k in range(5):
+        ga, gb = load(res_a / ("gder_%d.out" % k)), load(res_b / ("gder_%d.out" % k))
+        np.testing.assert_allclose(gb[:, 0], ga[:, 0], atol=1e-6)
+        # positions agree to ~1e-5, so a pair can change bin at a bin edge
+        diff = np.abs(gb[:, 1:] - ga[:, 1:])
+        assert diff.mean() < 5e-3, diff.mean()
+        assert (diff > 0.05).mean() < 0.01
+
+
+def test_cli_reproduces_reference_sample_counter_error(tmp_path):
+    a, b = tmp_path / "ref", tmp_path / "ours"
+    tree(a, 200, 200, 0.4, 1)
+    shutil.copytree(a, b)
+    data = BAD.replace("\n2\n100", "\n1\n100")
+    ra = subprocess.run([REF], input=data, cwd=a / "simulation", capture_output=True, text=True, timeout=600)
+    rb = subprocess.run([CLI], input=data, cwd=b / "simulation", capture_output=True, text=True, timeout=600)
+    assert ra.returncode == rb.returncode == 1
+    assert "ERROR: counter=6 fuera de rango" in ra.stderr
+    assert "ERROR: counter=6 fuera de rango" in rb.stderr

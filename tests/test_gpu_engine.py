@@ -136,3 +136,19 @@ def test_nan_temperature_of_instant_quench_is_reported():
     with pytest.raises(B.BDError) as ei:
         e.run(12)
     assert ei.value.code == 9
+
+
+def test_graph_relaunch_after_single_steps():
+    # 101 steps leave the buffer rotation one phase on (96 in a graph + 5 single
+    # steps); later graph launches must use the rotation they run in
+    s, pos = system(500, 700, 0.5, 15)
+    e1 = B.Engine([s], graph_steps=96)
+    e1.set_positions(pos)
+    e1.run(101)
+    e1.run(204)
+    e1.run(97)
+    e2 = B.Engine([s], graph_steps=96)
+    e2.set_positions(pos)
+    for _ in range(402):
+        e2.run(1)
+    np.testing.assert_array_equal(e1.get_positions()[0], e2.get_positions()[0])
