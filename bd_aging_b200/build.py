@@ -20,7 +20,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libbd_aging_b200.so")
 CLI = os.path.join(HERE, "bd_aging_self")
 
-SOURCES = ["mirror.cu", "engine.cu", "cv3d.cu", "noalloc.cu"]
+SOURCES = ["mirror.cu", "engine.cu", "correlate.cu", "gder.cu", "surrogate.cu", "cv3d.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
               "-I" + os.path.join(ROOT, "include"), "--expt-relaxed-constexpr"] + ARCH
@@ -42,7 +42,8 @@ def _newer(target: str, deps) -> bool:
 
 def _headers():
     hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
-    return hs + [os.path.join(ROOT, "include", "bd_aging.h")]
+    inc = os.path.join(ROOT, "include")
+    return hs + [os.path.join(inc, f) for f in os.listdir(inc) if f.endswith(".h")]
 
 
 def build(verbose: bool = False, ptxas_info: bool = False) -> str:

@@ -41,9 +41,53 @@ __device__ __forceinline__ float min_image_gder(float d, float side, float side_
     float t = __double2float_rn(__dadd_rn((double)__fmul_rn(side_inv, d), 0.5));
     return __fsub_rn(d, __fmul_rn(side, floorf(t)));
 }
+// min_image_gder with an exact shortcut: when |d / side| < 0.49 the floor
+// term is 0 and the result is d itself
+__device__ __forceinline__ float min_image_gder_fast(float d, float side, float side_inv) {
+    return fabsf(__fmul_rn(side_inv, d)) < 0.49f ? d : min_image_gder(d, side, side_inv);
+}
 // (dx*dx + dy*dy) + dz*dz, every operation rounded (reference host order)
 __device__ __forceinline__ float dist2_rn(float dx, float dy, float dz) {
     return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+}
+
+// ------------------------------------------------------------------ rannew64
+// rannew64 (rannew64.cu:55-126): subtractive lagged Fibonacci x[np] -= x[nq]
+// over a 250-word ring (taps 250 and 103, pointers walking down from 249 and
+// 102) minus a 64-bit LCG, uniform = (x - y) / (2^64 - 1) in double.  The
+// engine keeps one stream per particle; every particle draws 4 uniforms per
+// step, so the ring pointers are the same for all particles and follow from
+// the number of draws since seeding.
+constexpr unsigned long long kRnSeedA = 6364136223846793005ULL, kRnSeedC = 1442695040888963407ULL;
+constexpr unsigned long long kRnA = 2862933555777941757ULL, kRnC = 3037000493ULL;
+constexpr int kRnWords = 250, kRnDrawsPerStep = 4;
+
+__device__ __forceinline__ double rannew64_uniform(unsigned long long x, unsigned long long y) {
+    return (1.0 / 18446744073709551615.0) * __ull2double_rn(x - y);
+}
+// three N(0,1) values from the 4 draws of step `steps_done` (Box-Muller on
+// (u0, u1) and (u2, u3) in float, the sine of the second pair dropped)
+__device__ __forceinline__ float3 rannew64_gauss3(unsigned long long *ring, unsigned long long *lcg, int sid,
+                                                  size_t P, long long steps_done) {
+    const int d = (int)((steps_done * kRnDrawsPerStep) % kRnWords);
+    int np = 249 - d, nq = np - 147;
+    if (nq < 0) nq += kRnWords;
+    unsigned long long y = lcg[sid];
+    float u[kRnDrawsPerStep];
+#pragma unroll
+    for (int k = 0; k < kRnDrawsPerStep; k++) {
+        const unsigned long long x = ring[(size_t)np * P + sid] - ring[(size_t)nq * P + sid];
+        ring[(size_t)np * P + sid] = x;
+        np = np ? np - 1 : kRnWords - 1;
+        nq = nq ? nq - 1 : kRnWords - 1;
+        y = kRnA * y + kRnC;
+        u[k] = __double2float_rn(rannew64_uniform(x, y));
+    }
+    lcg[sid] = y;
+    const float r0 = sqrtf(-2.0f * logf(fmaxf(u[0], 1.17549435e-38f)));
+    const float r1 = sqrtf(-2.0f * logf(fmaxf(u[2], 1.17549435e-38f)));
+    const float t0 = __fmul_rn(6.2831853f, u[1]), t1 = __fmul_rn(6.2831853f, u[3]);
+    return make_float3(__fmul_rn(r0, cosf(t0)), __fmul_rn(r0, sinf(t0)), __fmul_rn(r1, cosf(t1)));
 }
 
 // ------------------------------------------------------------------ WCA pair

@@ -2,6 +2,7 @@
 // geometry, buffers, initial load, CUDA-graph stepping, observation passes,
 // export, and the batch g(r) kernel.
 #include "engine_kernels.cuh"
+#include "engine_state.cuh"
 
 namespace bd {
 
@@ -15,9 +16,9 @@ namespace bd {
 constexpr int kGrTile = 1024;
 __device__ __forceinline__ int gr_bin(float dx, float dy, float dz, float side, float side_inv, float range,
                                       float range2_hi, float bin_size, int nbins) {
-    dx = min_image_gder(dx, side, side_inv);
-    dy = min_image_gder(dy, side, side_inv);
-    dz = min_image_gder(dz, side, side_inv);
+    dx = min_image_gder_fast(dx, side, side_inv);
+    dy = min_image_gder_fast(dy, side, side_inv);
+    dz = min_image_gder_fast(dz, side, side_inv);
     float d2 = dist2_rn(dx, dy, dz);
     if (!(d2 <= range2_hi)) return -1;
     float dist = __fsqrt_rn(d2);
@@ -75,53 +76,7 @@ __global__ void __launch_bounds__(256) k_gr_batch(const float4 *__restrict__ sna
 
 using namespace bd;
 
-struct bd_engine {
-    int dev = 0;
-    cudaStream_t stream = nullptr;
-    int R = 0;
-    std::vector<bd_system_desc> desc;
-    std::vector<SysDev> sysh;
-    SysDev *d_sys = nullptr;
-    std::vector<int4> bricks_h;
-    int4 *d_bricks = nullptr;
-    int nbricks = 0;
-    int bx = 4, by = 4, bz = 3, cap = 16, threads = 128, smax = 0, mode = BD_MODE_PLAIN, cluster = 8;
-    size_t smem = 0, smem_census = 0;
-    long long C = 0, P = 0;
-    int *cnt[3] = {nullptr, nullptr, nullptr};
-    float4 *pos[3] = {nullptr, nullptr, nullptr};
-    int cur = 0;
-    float *lo[3] = {nullptr, nullptr, nullptr};
-    double *dsp[3] = {nullptr, nullptr, nullptr};
-    int *gid_of = nullptr, *rep_of_sid = nullptr, *rep_of_gid = nullptr;
-    double *x0 = nullptr, *obs = nullptr;
-    float4 *snap = nullptr;
-    int *nbr_count = nullptr;
-    unsigned long long *nbr_hash = nullptr;
-    curandState *cr = nullptr;
-    float *noise = nullptr;
-    unsigned *status = nullptr;
-    long long *d_ni = nullptr;
-    float *out_pos = nullptr, *out_raw = nullptr;
-    long long ni = 0, ni_first = 0;
-    int rng = BD_RNG_PHILOX;
-    unsigned rng_stream = 0;
-    float qmax = 6.2831853f;
-    bool loaded = false;
-    int graph_steps = 96;
-    cudaGraphExec_t gexec[3] = {nullptr, nullptr, nullptr};  // one per rotation phase e->cur
-    int autotune = 0;
-    bool tuned = false;
-};
-
 namespace {
-
-int engine_status(bd_engine *e) {
-    unsigned bits = 0;
-    BD_CUDA_TRY(cudaMemcpyAsync(&bits, e->status, sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream));
-    BD_CUDA_TRY(cudaStreamSynchronize(e->stream));
-    return status_from_bits(bits);
-}
 
 StepArgs make_args(bd_engine *e, int buf, int do_update) {
     StepArgs a;
@@ -148,11 +103,18 @@ StepArgs make_args(bd_engine *e, int buf, int do_update) {
     a.nbr_hash = e->nbr_hash;
     a.curand_states = e->cr;
     a.noise = e->noise;
+    a.rn_ring = e->rn_ring;
+    a.rn_lcg = e->rn_lcg;
+    a.rn_ni0 = e->rn_ni0;
     a.status = e->status;
     a.ni_first = e->ni_first;
     a.qmax = e->qmax;
     a.do_update = do_update;
     a.rng_stream = e->rng_stream;
+    for (int k = 0; k < 3; k++) { a.cnt3[k] = e->cnt[k]; a.pos3[k] = e->pos[k]; }
+    a.cur0 = buf % 3;
+    a.cl_start = e->d_cl_start;
+    a.cl_bricks = e->d_cl_bricks;
     return a;
 }
 
@@ -172,10 +134,67 @@ int launch_step_t(bd_engine *e, const StepArgs &a, int ni_off, bool attr_only = 
     return BD_OK;
 }
 
+template <int RNG>
+int launch_persistent_t(bd_engine *e, const StepArgs &a, int nsteps, bool attr_only = false) {
+    auto kern = k_step_persistent<RNG>;
+    if (attr_only) {
+        BD_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e->smem));
+        return BD_OK;
+    }
+    cudaLaunchConfig_t cfg;
+    std::memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3(e->nclusters * e->cluster);
+    cfg.blockDim = dim3(e->threads);
+    cfg.dynamicSmemBytes = e->smem;
+    cfg.stream = e->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = e->cluster;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    BD_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, a, (const long long *)e->d_ni, nsteps));
+    return BD_OK;
+}
+int launch_persistent(bd_engine *e, const StepArgs &a, int nsteps) {
+    switch (e->rng) {
+        case BD_RNG_CURAND: return launch_persistent_t<kRngCurand>(e, a, nsteps);
+        case BD_RNG_NOISE: return launch_persistent_t<kRngNoise>(e, a, nsteps);
+        case BD_RNG_RANNEW64: return launch_persistent_t<kRngRannew64>(e, a, nsteps);
+        default: return launch_persistent_t<kRngPhilox>(e, a, nsteps);
+    }
+}
+// Clusters of e->cluster CTAs that can be resident at once (0 if none).
+int max_active_clusters(bd_engine *e) {
+    cudaLaunchConfig_t cfg;
+    std::memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3(e->cluster);
+    cfg.blockDim = dim3(e->threads);
+    cfg.dynamicSmemBytes = e->smem;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = e->cluster;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k_step_persistent<kRngPhilox>, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
 int configure_kernels(bd_engine *e) {
     StepArgs a;
     std::memset(&a, 0, sizeof(a));
     int rc = 0;
+    rc |= launch_persistent_t<kRngPhilox>(e, a, 0, true);
+    rc |= launch_persistent_t<kRngCurand>(e, a, 0, true);
+    rc |= launch_persistent_t<kRngNoise>(e, a, 0, true);
+    rc |= launch_persistent_t<kRngRannew64>(e, a, 0, true);
 #define BD_ATTR(R)                                                 \
     rc |= launch_step_t<R, false, false>(e, a, 0, true);           \
     rc |= launch_step_t<R, true, false>(e, a, 0, true);            \
@@ -183,35 +202,35 @@ int configure_kernels(bd_engine *e) {
     BD_ATTR(kRngPhilox)
     BD_ATTR(kRngCurand)
     BD_ATTR(kRngNoise)
+    BD_ATTR(kRngRannew64)
 #undef BD_ATTR
     return rc ? BD_ERR_CUDA : BD_OK;
 }
 
+template <bool OBS, bool CENSUS>
+int launch_step_rng(bd_engine *e, const StepArgs &a, int ni_off) {
+    switch (e->rng) {
+        case BD_RNG_CURAND: return launch_step_t<kRngCurand, OBS, CENSUS>(e, a, ni_off);
+        case BD_RNG_NOISE: return launch_step_t<kRngNoise, OBS, CENSUS>(e, a, ni_off);
+        case BD_RNG_RANNEW64: return launch_step_t<kRngRannew64, OBS, CENSUS>(e, a, ni_off);
+        default: return launch_step_t<kRngPhilox, OBS, CENSUS>(e, a, ni_off);
+    }
+}
 int launch_step(bd_engine *e, const StepArgs &a, int ni_off, bool obs, bool census) {
-    if (census) {
-        if (e->rng == BD_RNG_CURAND) return launch_step_t<kRngCurand, false, true>(e, a, ni_off);
-        if (e->rng == BD_RNG_NOISE) return launch_step_t<kRngNoise, false, true>(e, a, ni_off);
-        return launch_step_t<kRngPhilox, false, true>(e, a, ni_off);
-    }
-    if (obs) {
-        if (e->rng == BD_RNG_CURAND) return launch_step_t<kRngCurand, true, false>(e, a, ni_off);
-        if (e->rng == BD_RNG_NOISE) return launch_step_t<kRngNoise, true, false>(e, a, ni_off);
-        return launch_step_t<kRngPhilox, true, false>(e, a, ni_off);
-    }
-    if (e->rng == BD_RNG_CURAND) return launch_step_t<kRngCurand, false, false>(e, a, ni_off);
-    if (e->rng == BD_RNG_NOISE) return launch_step_t<kRngNoise, false, false>(e, a, ni_off);
-    return launch_step_t<kRngPhilox, false, false>(e, a, ni_off);
+    if (census) return launch_step_rng<false, true>(e, a, ni_off);
+    if (obs) return launch_step_rng<true, false>(e, a, ni_off);
+    return launch_step_rng<false, false>(e, a, ni_off);
 }
 
-// one plain step (outside graphs): launch, advance the device counter
-int plain_step(bd_engine *e) {
+// k steps outside graphs (k = 1 in plain mode): launch, advance the counter
+int direct_steps(bd_engine *e, int k) {
     StepArgs a = make_args(e, e->cur, 1);
-    int rc = launch_step(e, a, 0, false, false);
+    int rc = e->mode == BD_MODE_PERSISTENT ? launch_persistent(e, a, k) : launch_step(e, a, 0, false, false);
     if (rc) return rc;
-    k_advance_counter<<<1, 1, 0, e->stream>>>(e->d_ni, 1);
+    k_advance_counter<<<1, 1, 0, e->stream>>>(e->d_ni, k);
     BD_LAUNCH_CHECK();
-    e->cur = (e->cur + 1) % 3;
-    e->ni += 1;
+    e->cur = (e->cur + k) % 3;
+    e->ni += k;
     return BD_OK;
 }
 
@@ -222,9 +241,14 @@ int build_graph(bd_engine *e) {
     cudaGraph_t g;
     BD_CUDA_TRY(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
     int rc = BD_OK;
-    for (int j = 0; j < e->graph_steps && rc == BD_OK; j++) {
-        StepArgs a = make_args(e, e->cur + j, 1);
-        rc = launch_step(e, a, j, false, false);
+    if (e->mode == BD_MODE_PERSISTENT) {
+        StepArgs a = make_args(e, e->cur, 1);
+        rc = launch_persistent(e, a, e->graph_steps);
+    } else {
+        for (int j = 0; j < e->graph_steps && rc == BD_OK; j++) {
+            StepArgs a = make_args(e, e->cur + j, 1);
+            rc = launch_step(e, a, j, false, false);
+        }
     }
     if (rc == BD_OK) k_advance_counter<<<1, 1, 0, e->stream>>>(e->d_ni, e->graph_steps);
     cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
@@ -241,11 +265,99 @@ void free_engine(bd_engine *e) {
     void *ptrs[] = {e->d_sys, e->d_bricks, e->cnt[0], e->cnt[1], e->cnt[2], e->pos[0], e->pos[1], e->pos[2],
                     e->lo[0], e->lo[1], e->lo[2], e->dsp[0], e->dsp[1], e->dsp[2], e->gid_of, e->rep_of_sid,
                     e->rep_of_gid, e->x0, e->obs, e->snap, e->nbr_count, e->nbr_hash, e->cr, e->noise,
-                    e->status, e->d_ni, e->out_pos, e->out_raw};
+                    e->status, e->d_ni, e->out_pos, e->out_raw, e->d_cl_start, e->d_cl_bricks, e->rn_ring, e->rn_lcg,
+                    e->snaps, e->d_segs, e->d_seg_first, e->corr_part, e->corr_out};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
+}
+
+// Brick decomposition of every replica for the current brick shape and CTA
+// size; in persistent mode also the packing of replicas into cluster bins
+// (longest-processing-time first by brick count).  Host side only.
+int rebuild_bricks(bd_engine *e) {
+    e->bricks_h.clear();
+    for (int r = 0; r < e->R; r++) {
+        SysDev &S = e->sysh[r];
+        const int nc = S.ncell;
+        S.nbx = (nc + e->bx - 1) / e->bx;
+        S.nby = (nc + e->by - 1) / e->by;
+        S.nbz = (nc + e->bz - 1) / e->bz;
+        S.brick_base = (int)e->bricks_h.size();
+        for (int z = 0; z < S.nbz; z++)
+            for (int y = 0; y < S.nby; y++)
+                for (int x = 0; x < S.nbx; x++) e->bricks_h.push_back(make_int4(r, x * e->bx, y * e->by, z * e->bz));
+    }
+    e->nbricks = (int)e->bricks_h.size();
+    const int nh = (e->bx + 2) * (e->by + 2) * (e->bz + 2);
+    // Staging capacity: the densest replica's mean cell occupancy over the
+    // halo block with 25% + 32 slots of headroom (a liquid's particle count
+    // in a few hundred cells varies by a few percent; a uniform random start
+    // by ~4%), never above what the cells can hold.
+    double occ = 0.0;
+    for (int r = 0; r < e->R; r++) {
+        const SysDev &S = e->sysh[r];
+        occ = std::max(occ, (double)S.n / ((double)S.ncell * S.ncell * S.ncell));
+    }
+    const long long want = (long long)std::ceil(occ * nh * 1.25) + 32;
+    e->smax = (int)std::min<long long>(std::min<long long>(65534, (long long)nh * e->cap), std::max(256LL, want)) & ~1;
+    e->smem = brick_smem_bytes(nh, e->smax, e->threads);
+    e->smem_census = e->smem;
+    if (e->smem > 227 * 1024 || nh > 65535) return BD_ERR_ARG;
+    e->cl_start_h.clear();
+    e->cl_bricks_h.clear();
+    if (e->mode == BD_MODE_PERSISTENT) {
+        const int G = std::max(1, std::min(e->R, e->max_clusters > 0 ? e->max_clusters : e->R));
+        std::vector<int> order(e->R);
+        std::iota(order.begin(), order.end(), 0);
+        auto nb_of = [&](int r) { const SysDev &S = e->sysh[r]; return S.nbx * S.nby * S.nbz; };
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return nb_of(a) > nb_of(b); });
+        std::vector<long long> load(G, 0);
+        std::vector<std::vector<int>> bins(G);
+        for (int r : order) {
+            int g = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+            bins[g].push_back(r);
+            load[g] += nb_of(r);
+        }
+        e->cl_start_h.push_back(0);
+        for (int g = 0; g < G; g++) {
+            std::sort(bins[g].begin(), bins[g].end());
+            for (int r : bins[g]) {
+                const SysDev &S = e->sysh[r];
+                for (int b = 0; b < nb_of(r); b++) e->cl_bricks_h.push_back(S.brick_base + b);
+            }
+            e->cl_start_h.push_back((int)e->cl_bricks_h.size());
+        }
+        e->nclusters = G;
+    }
+    return BD_OK;
+}
+
+// Upload the brick layout (after rebuild_bricks) and drop graphs recorded
+// for the previous layout.
+int upload_layout(bd_engine *e) {
+    for (int k = 0; k < 3; k++)
+        if (e->gexec[k]) { cudaGraphExecDestroy(e->gexec[k]); e->gexec[k] = nullptr; }
+    if (e->d_bricks) cudaFree(e->d_bricks);
+    e->d_bricks = nullptr;
+    BD_CUDA_TRY(cudaMalloc(&e->d_bricks, sizeof(int4) * e->nbricks));
+    BD_CUDA_TRY(cudaMemcpyAsync(e->d_bricks, e->bricks_h.data(), sizeof(int4) * e->nbricks, cudaMemcpyHostToDevice,
+                                e->stream));
+    BD_CUDA_TRY(cudaMemcpyAsync(e->d_sys, e->sysh.data(), sizeof(SysDev) * e->R, cudaMemcpyHostToDevice, e->stream));
+    if (e->d_cl_start) cudaFree(e->d_cl_start);
+    if (e->d_cl_bricks) cudaFree(e->d_cl_bricks);
+    e->d_cl_start = e->d_cl_bricks = nullptr;
+    if (e->mode == BD_MODE_PERSISTENT) {
+        BD_CUDA_TRY(cudaMalloc(&e->d_cl_start, sizeof(int) * e->cl_start_h.size()));
+        BD_CUDA_TRY(cudaMalloc(&e->d_cl_bricks, sizeof(int) * std::max<size_t>(1, e->cl_bricks_h.size())));
+        BD_CUDA_TRY(cudaMemcpyAsync(e->d_cl_start, e->cl_start_h.data(), sizeof(int) * e->cl_start_h.size(),
+                                    cudaMemcpyHostToDevice, e->stream));
+        BD_CUDA_TRY(cudaMemcpyAsync(e->d_cl_bricks, e->cl_bricks_h.data(), sizeof(int) * e->cl_bricks_h.size(),
+                                    cudaMemcpyHostToDevice, e->stream));
+    }
+    BD_CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return configure_kernels(e);
 }
 
 int setup_geometry(bd_engine *e) {
@@ -282,26 +394,13 @@ int setup_geometry(bd_engine *e) {
         S.protocol = d.temp_protocol;
         S.T0 = d.T0; S.Tf = d.Tf; S.t0 = d.t0; S.tf = d.tf; S.period = d.period;
         S.seed = d.seed;
-        S.nbx = (nc + e->bx - 1) / e->bx;
-        S.nby = (nc + e->by - 1) / e->by;
-        S.nbz = (nc + e->bz - 1) / e->bz;
-        S.brick_base = (int)e->bricks_h.size();
-        for (int z = 0; z < S.nbz; z++)
-            for (int y = 0; y < S.nby; y++)
-                for (int x = 0; x < S.nbx; x++) e->bricks_h.push_back(make_int4(r, x * e->bx, y * e->by, z * e->bz));
         cell_base += (long long)nc * nc * nc;
         part_base += S.n;
         if (cell_base > (1ll << 31) / e->cap || part_base >= (1ll << 31)) return BD_ERR_ARG;
     }
     e->C = cell_base;
     e->P = part_base;
-    e->nbricks = (int)e->bricks_h.size();
-    const int nh = (e->bx + 2) * (e->by + 2) * (e->bz + 2);
-    e->smax = std::min(65534, std::max(256, (7 * nh) / 2)) & ~1;  // even: 8-byte aligned views
-    e->smem = brick_smem_bytes(nh, e->smax, e->threads);
-    e->smem_census = e->smem;
-    if (e->smem_census > 227 * 1024) return BD_ERR_ARG;
-    return BD_OK;
+    return rebuild_bricks(e);
 }
 
 }  // namespace
@@ -329,7 +428,7 @@ int bd_engine_create(const bd_system_desc *systems, int nsys, const bd_engine_op
     e->R = nsys;
     e->desc.assign(systems, systems + nsys);
     e->rng = opts.rng;
-    if (e->rng < 0 || e->rng > 2) { delete e; return BD_ERR_ARG; }
+    if (e->rng < BD_RNG_PHILOX || e->rng > BD_RNG_RANNEW64) { delete e; return BD_ERR_ARG; }
     e->cap = opts.cell_capacity > 0 ? opts.cell_capacity : 16;
     if (e->cap > kQueue / 3) { delete e; return BD_ERR_ARG; }  // a row of 3 cells must fit one queue
     if (opts.brick[0] > 0 && opts.brick[1] > 0 && opts.brick[2] > 0) {
@@ -373,6 +472,10 @@ int bd_engine_create(const bd_system_desc *systems, int nsys, const bd_engine_op
     ALLOC(e->d_ni, sizeof(long long));
     if (e->rng == BD_RNG_CURAND) ALLOC(e->cr, sizeof(curandState) * P);
     if (e->rng == BD_RNG_NOISE) ALLOC(e->noise, sizeof(float) * 3 * P);
+    if (e->rng == BD_RNG_RANNEW64) {
+        ALLOC(e->rn_ring, sizeof(unsigned long long) * kRnWords * P);
+        ALLOC(e->rn_lcg, sizeof(unsigned long long) * P);
+    }
 #undef ALLOC
     cudaMemcpyAsync(e->d_sys, e->sysh.data(), sizeof(SysDev) * e->R, cudaMemcpyHostToDevice, e->stream);
     cudaMemcpyAsync(e->d_bricks, e->bricks_h.data(), sizeof(int4) * e->nbricks, cudaMemcpyHostToDevice, e->stream);
@@ -388,6 +491,12 @@ int bd_engine_create(const bd_system_desc *systems, int nsys, const bd_engine_op
     if (configure_kernels(e) != BD_OK) {
         free_engine(e);
         return BD_ERR_CUDA;
+    }
+    if (e->mode == BD_MODE_PERSISTENT) {  // as many cluster bins as can be resident at once
+        if (e->cluster < 1 || e->cluster > 8) { free_engine(e); return BD_ERR_ARG; }
+        e->max_clusters = max_active_clusters(e);
+        if (e->max_clusters < 1) { free_engine(e); return BD_ERR_ARG; }
+        if (rebuild_bricks(e) != BD_OK || upload_layout(e) != BD_OK) { free_engine(e); return BD_ERR_CUDA; }
     }
     if (cudaStreamSynchronize(e->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
         free_engine(e);
@@ -484,8 +593,17 @@ int bd_engine_set_positions(bd_engine *e, const float *pos) {
     }
     cudaMemsetAsync(e->status, 0, 256, e->stream);
     e->cur = 0;
+    e->generation++;  // displacement snapshots of earlier positions are void
+    if (e->rng == BD_RNG_RANNEW64) {  // streams keyed by particle, stored by storage id
+        e->rn_ni0 = e->ni;
+        for (int g = 0; g < 3; g++)
+            if (e->gexec[g]) { cudaGraphExecDestroy(e->gexec[g]); e->gexec[g] = nullptr; }
+    }
     k_load<<<div_up((long)P, 256), 256, 0, e->stream>>>(d_staged, (int)P, e->rep_of_sid, e->d_sys, e->cnt[0],
                                                         e->pos[0], e->cap, e->x0, e->gid_of, e->status);
+    if (e->rng == BD_RNG_RANNEW64)
+        k_rannew64_seed<<<div_up((long)P, 128), 128, 0, e->stream>>>(e->rn_ring, e->rn_lcg, e->d_sys, e->rep_of_sid,
+                                                                     e->gid_of, (int)P);
     cudaError_t le = cudaGetLastError();
     cudaStreamSynchronize(e->stream);
     cudaFree(d_staged);
@@ -495,10 +613,91 @@ int bd_engine_set_positions(bd_engine *e, const float *pos) {
     return engine_status(e);
 }
 
+}  // extern "C"
+
+namespace {
+// Steps issued directly (no graph): one persistent launch, or k plain launches.
+int run_direct(bd_engine *e, int k) {
+    if (k <= 0) return BD_OK;
+    if (e->mode == BD_MODE_PERSISTENT) return direct_steps(e, k);
+    for (int i = 0; i < k; i++) {
+        int rc = direct_steps(e, 1);
+        if (rc) return rc;
+    }
+    return BD_OK;
+}
+
+// Project autotuner: times brick shapes x CTA sizes (and cluster sizes in
+// persistent mode) on the live batch and keeps the fastest.  The steps it
+// takes are real steps of the run; results do not depend on the layout
+// (every force sum has a fixed order), only the speed does.
+int autotune_layout(bd_engine *e, long long &nsteps) {
+    struct Cand { int bx, by, bz, t, cl; };
+    static const int shapes[][4] = {{4, 4, 3, 128}, {4, 4, 4, 160}, {5, 4, 4, 192}, {4, 3, 3, 96}, {3, 3, 3, 64},
+                                    {4, 4, 2, 96},  {2, 2, 2, 64},  {3, 3, 2, 64},  {6, 4, 3, 192}};
+    std::vector<Cand> cands;
+    for (auto &s : shapes) {
+        if (e->mode == BD_MODE_PERSISTENT) {
+            for (int cl : {8, 4, 2}) cands.push_back({s[0], s[1], s[2], s[3], cl});
+        } else {
+            cands.push_back({s[0], s[1], s[2], s[3], e->cluster});
+        }
+    }
+    const int warm = 2, timed = 6;
+    if (nsteps < (long long)cands.size() * (warm + timed) + 1) return BD_OK;  // too short to tune now
+    cudaEvent_t t0, t1;
+    BD_CUDA_TRY(cudaEventCreate(&t0));
+    BD_CUDA_TRY(cudaEventCreate(&t1));
+    const Cand orig = {e->bx, e->by, e->bz, e->threads, e->cluster};
+    Cand best = orig;
+    float best_ms = 1e30f;
+    int rc = BD_OK;
+    for (const Cand &c : cands) {
+        e->bx = c.bx; e->by = c.by; e->bz = c.bz; e->threads = c.t; e->cluster = c.cl;
+        if (rebuild_bricks(e) != BD_OK) continue;
+        if (e->mode == BD_MODE_PERSISTENT) {
+            if ((rc = configure_kernels(e)) != BD_OK) break;
+            e->max_clusters = max_active_clusters(e);
+            if (e->max_clusters < 1 || rebuild_bricks(e) != BD_OK) continue;
+        }
+        if ((rc = upload_layout(e)) != BD_OK) break;
+        if ((rc = run_direct(e, warm)) != BD_OK) break;
+        BD_CUDA_TRY(cudaEventRecord(t0, e->stream));
+        if ((rc = run_direct(e, timed)) != BD_OK) break;
+        BD_CUDA_TRY(cudaEventRecord(t1, e->stream));
+        if ((rc = engine_status(e)) != BD_OK) break;
+        float ms = 0.f;
+        BD_CUDA_TRY(cudaEventElapsedTime(&ms, t0, t1));
+        nsteps -= warm + timed;
+        if (ms < best_ms) { best_ms = ms; best = c; }
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (rc) return rc;
+    e->bx = best.bx; e->by = best.by; e->bz = best.bz; e->threads = best.t; e->cluster = best.cl;
+    if ((rc = rebuild_bricks(e)) != BD_OK) return rc;
+    if (e->mode == BD_MODE_PERSISTENT) {
+        if ((rc = configure_kernels(e)) != BD_OK) return rc;
+        e->max_clusters = max_active_clusters(e);
+        if ((rc = rebuild_bricks(e)) != BD_OK) return rc;
+    }
+    if ((rc = upload_layout(e)) != BD_OK) return rc;
+    e->tuned = true;
+    e->tuned_ms = best_ms / timed;
+    return BD_OK;
+}
+}  // namespace
+
+extern "C" {
+
 int bd_engine_run(bd_engine *e, long long nsteps) {
     if (!e || nsteps < 0) return BD_ERR_ARG;
     if (!e->loaded) return BD_ERR_STATE;
     if (e->rng == BD_RNG_NOISE && nsteps > 1) return BD_ERR_ARG;  // one injected step at a time
+    if (e->autotune && !e->tuned && e->rng != BD_RNG_NOISE) {
+        int rc = autotune_layout(e, nsteps);
+        if (rc) return rc;
+    }
     while (nsteps > 0) {
         if (nsteps >= e->graph_steps && e->rng != BD_RNG_NOISE) {
             int rc = build_graph(e);
@@ -507,9 +706,9 @@ int bd_engine_run(bd_engine *e, long long nsteps) {
             e->ni += e->graph_steps;  // cur unchanged: graph_steps is a multiple of 3
             nsteps -= e->graph_steps;
         } else {
-            int rc = plain_step(e);
+            int rc = run_direct(e, (int)nsteps);
             if (rc) return rc;
-            nsteps -= 1;
+            nsteps = 0;
         }
     }
     return engine_status(e);
@@ -567,32 +766,55 @@ int bd_engine_get_positions(bd_engine *e, float *pos_host, float *raw_host) {
     return engine_status(e);
 }
 
-int bd_engine_gder(bd_engine *e, int nbins, float range, unsigned long long *counts_host) {
+int bd_engine_gder_method(bd_engine *e, int nbins, float range, int method, unsigned long long *counts_host) {
     if (!e || !counts_host || nbins < 1 || nbins > 4096 || !(range > 0)) return BD_ERR_ARG;
+    if (method != BD_GDER_AUTO && method != BD_GDER_ALL_PAIRS && method != BD_GDER_CELLS) return BD_ERR_ARG;
     if (!e->loaded) return BD_ERR_STATE;
-    k_export<<<div_up(e->C, 128), 128, 0, e->stream>>>(e->cnt[e->cur], e->pos[e->cur], (int)e->C, e->cap, (int)e->P, e->gid_of,
-                                                       e->x0, e->dsp[0], e->dsp[1], e->dsp[2], nullptr, nullptr,
-                                                       e->snap);
-    BD_LAUNCH_CHECK();
+    // per replica: cell-bounded when the stencil region is well inside the box
+    std::vector<int> m_of(e->R, -1);
+    bool any_all = false;
+    for (int r = 0; r < e->R; r++) {
+        const SysDev &S = e->sysh[r];
+        const int m = gder_cell_reach(S, range);
+        if (method == BD_GDER_CELLS && m < 0) return BD_ERR_ARG;
+        const double reg = (double)(4 + 2 * m), box = (double)S.ncell;
+        const bool cells = m >= 0 && (method == BD_GDER_CELLS || (method == BD_GDER_AUTO && reg * reg * reg <= 0.6 * box * box * box));
+        m_of[r] = cells ? m : -1;
+        any_all |= !cells;
+    }
     unsigned long long *d_counts = nullptr;
     const size_t per = (size_t)4 * nbins;
     BD_CUDA_TRY(cudaMalloc(&d_counts, sizeof(unsigned long long) * per * e->R));
     cudaMemsetAsync(d_counts, 0, sizeof(unsigned long long) * per * e->R, e->stream);
-    const size_t sm = kGrTile * sizeof(float4) + per * sizeof(unsigned);
-    cudaFuncSetAttribute(k_gr_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    const int jchunk = 8192;
-    for (int r = 0; r < e->R; r++) {
-        const SysDev &S = e->sysh[r];
-        dim3 grid(div_up(S.n, 256), div_up(S.n, jchunk));
-        k_gr_batch<<<grid, 256, sm, e->stream>>>(e->snap + S.part_base, S.n, S.n_big, S.L, range, nbins, jchunk,
-                                                 d_counts + per * r);
+    int rc = launch_gder_cells(e, m_of, nbins, range, d_counts);  // may hand replicas back
+    for (int r = 0; r < e->R; r++) any_all |= m_of[r] < 0;
+    cudaError_t le = cudaSuccess;
+    if (rc == BD_OK && any_all) {
+        k_export<<<div_up(e->C, 128), 128, 0, e->stream>>>(e->cnt[e->cur], e->pos[e->cur], (int)e->C, e->cap, (int)e->P,
+                                                           e->gid_of, e->x0, e->dsp[0], e->dsp[1], e->dsp[2], nullptr,
+                                                           nullptr, e->snap);
+        const size_t sm = kGrTile * sizeof(float4) + per * sizeof(unsigned);
+        cudaFuncSetAttribute(k_gr_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        const int jchunk = 8192;
+        for (int r = 0; r < e->R; r++) {
+            if (m_of[r] >= 0) continue;
+            const SysDev &S = e->sysh[r];
+            dim3 grid(div_up(S.n, 256), div_up(S.n, jchunk));
+            k_gr_batch<<<grid, 256, sm, e->stream>>>(e->snap + S.part_base, S.n, S.n_big, S.L, range, nbins, jchunk,
+                                                     d_counts + per * r);
+        }
+        le = cudaGetLastError();
+        if (le != cudaSuccess) rc = BD_ERR_CUDA;
     }
-    cudaError_t le = cudaGetLastError();
     cudaMemcpyAsync(counts_host, d_counts, sizeof(unsigned long long) * per * e->R, cudaMemcpyDeviceToHost, e->stream);
     cudaStreamSynchronize(e->stream);
     cudaFree(d_counts);
-    if (le != cudaSuccess) return BD_ERR_CUDA;
+    if (rc) return rc;
     return engine_status(e);
+}
+
+int bd_engine_gder(bd_engine *e, int nbins, float range, unsigned long long *counts_host) {
+    return bd_engine_gder_method(e, nbins, range, BD_GDER_AUTO, counts_host);
 }
 
 int bd_engine_set_noise(bd_engine *e, const float *noise_host) {

@@ -50,7 +50,7 @@ enum ObsField {
     kObsCount = 8
 };
 
-enum RngMode { kRngPhilox = 0, kRngCurand = 1, kRngNoise = 2 };
+enum RngMode { kRngPhilox = 0, kRngCurand = 1, kRngNoise = 2, kRngRannew64 = 3 };
 
 // candidates of one home cell held in registers per chunk (4 per lane)
 constexpr int kMaxCand = 128;
@@ -78,7 +78,15 @@ struct StepArgs {
     unsigned long long *nbr_hash;
     void *curand_states; // by gid
     const float *noise;  // [3P] by gid
+    unsigned long long *rn_ring;  // rannew64 mode: [250][P] lagged-Fibonacci words by storage id
+    unsigned long long *rn_lcg;   //   [P] LCG state by storage id
+    long long rn_ni0;             //   step index at which the streams were seeded
     unsigned *status;
+    int *cnt3[3];        // all three count / position buffers (persistent mode
+    float4 *pos3[3];     //   rotates them itself, step s uses (cur0 + s) % 3)
+    int cur0;
+    const int *cl_start; // persistent mode: bricks of cluster c are
+    const int *cl_bricks;//   cl_bricks[cl_start[c] .. cl_start[c+1])
     long long ni;        // reference step index of this update
     long long ni_first;  // first step of the run (the reference uses T0 there)
     float qmax;          // wave number of the built-in F_s accumulator

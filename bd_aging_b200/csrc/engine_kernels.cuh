@@ -158,6 +158,25 @@ __global__ void k_export(const int *__restrict__ cnt, const float4 *__restrict__
         if (snap) snap[gid] = make_float4(v.x, v.y, v.z, __int_as_float((int)(w >> 31)));
     }
 }
+// Per-particle rannew64 seeding (rannew64.cu, first call): particle pid of a
+// replica with seed S uses idum = S + pid (absolute value), 1000 warm-up LCG
+// steps, then 250 ring words; the second LCG starts from the last word.
+__global__ void k_rannew64_seed(unsigned long long *ring, unsigned long long *lcg, const SysDev *sys,
+                                const int *rep_of_sid, const int *gid_of, int P) {
+    const int sid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sid >= P) return;
+    const SysDev &S = sys[rep_of_sid[sid]];
+    long long idum = (long long)S.seed + (long long)(gid_of[sid] - S.part_base);
+    if (idum < 0) idum = -idum;
+    unsigned long long u = (unsigned long long)idum;
+    for (int i = 0; i < 1000; i++) u = u * kRnSeedA + kRnSeedC;
+    for (int i = 0; i < kRnWords; i++) {
+        u = u * kRnSeedA + kRnSeedC;
+        ring[(size_t)i * P + sid] = u;
+    }
+    lcg[sid] = u;
+}
+
 __global__ void k_curand_setup(curandState *st, const SysDev *sys, const int *rep_of_gid, int P) {
     int gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= P) return;

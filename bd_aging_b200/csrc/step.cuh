@@ -366,6 +366,8 @@ __device__ void process_brick(const StepArgs &a, int bidx, long long ni, unsigne
             xi.y = curand_normal(&st);
             xi.z = curand_normal(&st);
             *stp = st;
+        } else if (RNG == kRngRannew64) {
+            xi = rannew64_gauss3(a.rn_ring, a.rn_lcg, sid, (size_t)a.np, ni - a.rn_ni0);
         } else {
             xi = make_float3(a.noise[3 * (size_t)gid], a.noise[3 * (size_t)gid + 1], a.noise[3 * (size_t)gid + 2]);
         }
@@ -429,6 +431,38 @@ __global__ void __launch_bounds__(192, 4) k_step(StepArgs a, const long long *ni
     extern __shared__ __align__(16) unsigned char smem[];
     const long long ni = *ni_base + ni_off;
     process_brick<RNG, OBS, CENSUS>(a, blockIdx.x, ni, smem);
+}
+
+// Persistent mode: each thread-block cluster owns the bricks of a bin of
+// replicas and advances them `nsteps` time steps in one launch; between
+// steps the cluster synchronises with the hardware cluster barrier
+// (release/acquire at cluster scope orders the global-memory count and
+// position buffers, which are read and written at L2 with .cg accesses).
+// Replicas never span clusters, so no other synchronisation is needed.
+// Every CTA of a cluster executes the same number of barriers.
+template <int RNG>
+__global__ void __launch_bounds__(192, 4) k_step_persistent(StepArgs a, const long long *ni_base, int nsteps) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    unsigned cid, rank, csz;
+    asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(cid));
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(csz));
+    const long long ni0 = *ni_base;
+    const int b0 = a.cl_start[cid], b1 = a.cl_start[cid + 1];
+    for (int s = 0; s < nsteps; s++) {
+        StepArgs as = a;
+        const int c = (a.cur0 + s) % 3;
+        as.cnt_in = a.cnt3[c];
+        as.pos_in = a.pos3[c];
+        as.cnt_out = a.cnt3[(c + 1) % 3];
+        as.pos_out = a.pos3[(c + 1) % 3];
+        as.cnt_clr = a.cnt3[(c + 2) % 3];
+        for (int b = b0 + (int)rank; b < b1; b += (int)csz) {
+            process_brick<RNG, false, false>(as, a.cl_bricks[b], ni0 + s, smem);
+            __syncthreads();
+        }
+        asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+    }
 }
 
 }  // namespace bd

@@ -18,12 +18,14 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libbd_aging_b200.so")
 
-BD_OK = 0
+BD_OK, BD_ERR_ARG, BD_ERR_CUDA, BD_ERR_CELL_OVERFLOW, BD_ERR_NOMEM, BD_ERR_STATE = 0, 1, 2, 3, 4, 5
+BD_ERR_TIMEOUT, BD_ERR_FILE, BD_ERR_FORMAT, BD_ERR_NUMERIC = 6, 7, 8, 9
 STATUS_NAMES = {0: "BD_OK", 1: "BD_ERR_ARG", 2: "BD_ERR_CUDA", 3: "BD_ERR_CELL_OVERFLOW", 4: "BD_ERR_NOMEM",
                 5: "BD_ERR_STATE", 6: "BD_ERR_TIMEOUT", 7: "BD_ERR_FILE", 8: "BD_ERR_FORMAT", 9: "BD_ERR_NUMERIC"}
 PROTOCOL = {"linear": 0, "sine": 1, "const": 2}
-RNG = {"philox": 0, "curand": 1, "noise": 2}
+RNG = {"philox": 0, "curand": 1, "noise": 2, "rannew64": 3}
 MODE = {"auto": 0, "plain": 1, "persistent": 2}
+GDER = {"auto": 0, "all_pairs": 1, "cells": 2}
 
 
 class BDError(RuntimeError):
@@ -64,6 +66,16 @@ class Observables(C.Structure):
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class Correlation(C.Structure):
+    _fields_ = [("lag_steps", C.c_longlong)] + [(n, C.c_double) for n in ("fself_big", "fself_sml", "msd_big",
+                                                                         "msd_sml", "r4_big", "r4_sml")]
+
+
+CORR_DTYPE = np.dtype([("lag_steps", np.int64), ("fself_big", np.float64), ("fself_sml", np.float64),
+                       ("msd_big", np.float64), ("msd_sml", np.float64), ("r4_big", np.float64),
+                       ("r4_sml", np.float64)])
 
 
 class EngineInfo(C.Structure):
@@ -119,8 +131,25 @@ def _lib():
             "bd_engine_observe": ([_vp, C.POINTER(Observables)], C.c_int),
             "bd_engine_get_positions": ([_vp, _vp, _vp], C.c_int),
             "bd_engine_gder": ([_vp, C.c_int, C.c_float, _vp], C.c_int),
+            "bd_engine_gder_method": ([_vp, C.c_int, C.c_float, C.c_int, _vp], C.c_int),
             "bd_engine_set_noise": ([_vp, _vp], C.c_int),
             "bd_engine_census": ([_vp, _vp, _vp], C.c_int),
+            "bd_engine_reserve_snapshots": ([_vp, C.c_int], C.c_int),
+            "bd_engine_snapshot": ([_vp, C.c_int], C.c_int),
+            "bd_engine_correlate": ([_vp, _vp, C.c_int, C.c_double, _vp], C.c_int),
+            "bd_engine_get_displacements": ([_vp, _vp], C.c_int),
+            "bd_surrogate_create": ([C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_ulonglong, _vp], C.c_int),
+            "bd_surrogate_destroy": ([_vp], C.c_int),
+            "bd_surrogate_get_stream": ([_vp, _vp], C.c_int),
+            "bd_surrogate_param_count": ([_vp, _vp], C.c_int),
+            "bd_surrogate_get_params": ([_vp, _vp], C.c_int),
+            "bd_surrogate_set_params": ([_vp, _vp], C.c_int),
+            "bd_surrogate_set_output_weights": ([_vp, _vp], C.c_int),
+            "bd_surrogate_set_data": ([_vp, _vp, _vp, C.c_int], C.c_int),
+            "bd_surrogate_train": ([_vp, C.c_int, C.c_float, _vp], C.c_int),
+            "bd_surrogate_gradients": ([_vp, _vp, _vp, _vp, _vp], C.c_int),
+            "bd_surrogate_predict": ([_vp, _vp, C.c_int, _vp], C.c_int),
+            "bd_umma_gemm_bf16": ([_vp, _vp, C.c_int, C.c_int, C.c_int, _vp], C.c_int),
         }
         for name, (args, res) in sig.items():
             if hasattr(L, name):
@@ -376,9 +405,11 @@ class Engine:
         _check(_lib().bd_engine_get_positions(self._h, _ptr(pos), _ptr(raw)), "get_positions")
         return pos, raw
 
-    def gder(self, nbins: int, range_: float) -> np.ndarray:
+    def gder(self, nbins: int, range_: float, method: str = "auto") -> np.ndarray:
+        """Exact g(r) counts [nsys, 4 (bb, bs, sb, ss), nbins]; method "auto",
+        "all_pairs" or "cells" (same counts, different candidate search)."""
         out = np.zeros((len(self.systems), 4, nbins), np.uint64)
-        _check(_lib().bd_engine_gder(self._h, nbins, range_, _ptr(out)), "gder")
+        _check(_lib().bd_engine_gder_method(self._h, nbins, range_, GDER[method], _ptr(out)), "gder")
         return out
 
     def set_noise(self, noise: np.ndarray):
@@ -391,6 +422,27 @@ class Engine:
         _check(_lib().bd_engine_census(self._h, _ptr(cnt), _ptr(hsh)), "census")
         return cnt, hsh
 
+    def reserve_snapshots(self, nslots: int):
+        _check(_lib().bd_engine_reserve_snapshots(self._h, int(nslots)), "reserve_snapshots")
+
+    def snapshot(self, slot: int):
+        """Record every particle's displacement now (waiting time t_w) in `slot`."""
+        _check(_lib().bd_engine_snapshot(self._h, int(slot)), "snapshot")
+
+    def correlate(self, slots, q: float) -> np.ndarray:
+        """F_s(q), MSD and <|dr|^4> per species since each slot: array [len(slots), nsys]."""
+        sl = np.ascontiguousarray(np.atleast_1d(slots), np.int32)
+        out = np.zeros((len(sl), len(self.systems)), CORR_DTYPE)
+        assert CORR_DTYPE.itemsize == C.sizeof(Correlation)
+        _check(_lib().bd_engine_correlate(self._h, _ptr(sl), len(sl), float(q), _ptr(out)), "correlate")
+        return out
+
+    def get_displacements(self) -> np.ndarray:
+        """FP64 displacement since the origin step, [P, 3] in the set_positions order."""
+        out = np.zeros((self.P, 3), np.float64)
+        _check(_lib().bd_engine_get_displacements(self._h, _ptr(out)), "get_displacements")
+        return out
+
     def close(self):
         if getattr(self, "_h", None):
             _lib().bd_engine_destroy(self._h)
@@ -401,3 +453,89 @@ class Engine:
             self.close()
         except Exception:
             pass
+
+
+# ------------------------------------------------------------------ surrogate
+class Surrogate:
+    """The learned surrogate (bd_surrogate_*): MLP n_in -> width x depth (GELU)
+    -> n_out on tcgen05 BF16 GEMMs, FP32 Adam."""
+
+    def __init__(self, n_in=5, n_out=34, width=256, depth=4, batch=4096, seed=1):
+        L = _lib()
+        h = _vp()
+        _check(L.bd_surrogate_create(n_in, n_out, width, depth, batch, C.c_ulonglong(seed), C.byref(h)),
+               "bd_surrogate_create")
+        self._h = h
+        self.n_in, self.n_out, self.width, self.depth, self.batch = n_in, n_out, width, depth, batch
+        c = C.c_longlong(0)
+        _check(L.bd_surrogate_param_count(h, C.byref(c)), "param_count")
+        self.n_params = c.value
+
+    def sizes(self):
+        return [(self.width, self.n_in)] + [(self.width, self.width)] * (self.depth - 1) + \
+            [(self.n_out, self.width)]
+
+    def get_params(self) -> np.ndarray:
+        out = np.zeros(self.n_params, np.float32)
+        _check(_lib().bd_surrogate_get_params(self._h, _ptr(out)), "get_params")
+        return out
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.n_params
+        _check(_lib().bd_surrogate_set_params(self._h, _ptr(p)), "set_params")
+
+    def set_output_weights(self, w: np.ndarray):
+        w = np.ascontiguousarray(w, np.float32)
+        _check(_lib().bd_surrogate_set_output_weights(self._h, _ptr(w)), "set_output_weights")
+
+    def set_data(self, x: np.ndarray, y: np.ndarray):
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, self.n_in)
+        y = np.ascontiguousarray(y, np.float32).reshape(-1, self.n_out)
+        _check(_lib().bd_surrogate_set_data(self._h, _ptr(x), _ptr(y), len(x)), "set_data")
+
+    def train(self, steps: int, lr: float = 1e-3) -> float:
+        loss = C.c_float(0)
+        _check(_lib().bd_surrogate_train(self._h, int(steps), C.c_float(lr), C.byref(loss)), "train")
+        return loss.value
+
+    def gradients(self, x: np.ndarray, y: np.ndarray):
+        x = np.ascontiguousarray(x, np.float32).reshape(self.batch, self.n_in)
+        y = np.ascontiguousarray(y, np.float32).reshape(self.batch, self.n_out)
+        g = np.zeros(self.n_params, np.float32)
+        loss = C.c_float(0)
+        _check(_lib().bd_surrogate_gradients(self._h, _ptr(x), _ptr(y), _ptr(g), C.byref(loss)), "gradients")
+        return g, loss.value
+
+    def predict(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, self.n_in)
+        y = np.zeros((len(x), self.n_out), np.float32)
+        _check(_lib().bd_surrogate_predict(self._h, _ptr(x), len(x), _ptr(y)), "predict")
+        return y
+
+    def stream_handle(self) -> int:
+        s = _vp()
+        _check(_lib().bd_surrogate_get_stream(self._h, C.byref(s)), "get_stream")
+        return s.value or 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib().bd_surrogate_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def umma_gemm_bf16(a_bits: np.ndarray, b_bits: np.ndarray) -> np.ndarray:
+    """C = A B^T through the surrogate's tcgen05 GEMM kernel (BF16 bits in, FP32 out)."""
+    a_bits = np.ascontiguousarray(a_bits, np.uint16)
+    b_bits = np.ascontiguousarray(b_bits, np.uint16)
+    M, K = a_bits.shape
+    N = b_bits.shape[0]
+    c = np.zeros((M, N), np.float32)
+    _check(_lib().bd_umma_gemm_bf16(_ptr(a_bits), _ptr(b_bits), M, N, K, _ptr(c)), "umma_gemm_bf16")
+    return c

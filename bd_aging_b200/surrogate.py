@@ -1,0 +1,235 @@
+"""Learned surrogate of the aging observables, trained on the engine's own
+runs, and the proposal loop that uses it.
+
+The network (bd_surrogate_*, hand-written tcgen05 BF16 GEMMs) maps a setting
+    (phi, T_final, log10 t_w, log10 t, k)
+to 34 outputs: F_s(k; t_w, t_w + t) of the big particles, log10 MSD of the
+big particles over the same window, and 32 samples of the total g(r) at time
+t_w + t.  The reference has no learned component; the engine is both the
+source of the training data and the judge of every proposal: a proposed
+setting is always simulated before it is used.
+
+Proposal task.  For a fixed (phi, t_w, t, k), find the quench temperature
+T* at which F_s falls to a target value (0.5 by default): the temperature
+at which the structure relaxes within the observation window.  Without the
+surrogate the simulation budget goes on a uniform temperature grid; with it,
+each new simulation goes where the current network puts the crossing.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+from . import configs as CF
+from . import lib as B
+
+N_OUT = 34
+G_BINS = 32
+G_RANGE = (0.8, 2.4)  # r window of the g(r) features, in units of the small reference sigma
+
+
+# ------------------------------------------------------------------ data
+def make_systems(settings, n_per_replica=1000, dt=1e-4, seed=1):
+    """One replica per (phi, T_final): 50:50 mixture quenched from T0 = 1.0
+    to T_final at t = 0 (instantaneous: tf = t0 + 1e-30)."""
+    out = []
+    for i, (phi, tfin) in enumerate(settings):
+        nb = ns = n_per_replica // 2
+        side = float(np.float32(CF.side_from_phi(nb, ns, float(phi))))
+        out.append(B.System(n_big=nb, n_sml=ns, side=side, sigma_big=float(CF.SIGMA_BIG),
+                            sigma_sml=float(CF.SIGMA_SML), dt=dt, T0=1.0, Tf=float(tfin), t0=0.0, tf=1e-30,
+                            protocol="linear", seed=seed * 7919 + i))
+    return out
+
+
+def relaxed_start(systems, seed, relax_steps=1500):
+    """Uniform random positions relaxed together by capped-force steps."""
+    pos = np.concatenate([CF.uniform_config(s.n_big, s.n_sml, s.side, seed + k) for k, s in enumerate(systems)])
+    relax = [dataclasses.replace(s, dt=1e-4, protocol="const", T0=1.0, force_cap=100.0) for s in systems]
+    e = B.Engine(relax, rng_stream=1)
+    e.set_positions(pos)
+    e.run(relax_steps)
+    p, _ = e.get_positions()
+    e.close()
+    return p
+
+
+def g_features(counts, systems):
+    """Total g(r) at G_BINS points in G_RANGE from exact counts [R, 4, bins]
+    (bins of width (G_RANGE[1]) / nbins starting at 0)."""
+    nb = counts.shape[-1]
+    width = G_RANGE[1] / nb
+    r_lo = np.arange(nb) * width
+    shell = 4.0 / 3.0 * math.pi * ((r_lo + width) ** 3 - r_lo ** 3)
+    out = []
+    for r, s in enumerate(systems):
+        tot = counts[r].sum(0).astype(np.float64)
+        rho = s.n / s.side ** 3
+        g = tot / (s.n * rho * shell)
+        out.append(g[nb - G_BINS:])
+    return np.array(out)
+
+
+def simulate(settings, t_ws, lags, ks, n_per_replica=1000, dt=1e-4, trans_steps=200, seed=1, relax_steps=1500):
+    """Run one replica per setting through every (t_w, lag) and return
+    (X [samples, 5], Y [samples, 34]).  t_ws and lags are in steps; ks are
+    wave numbers.  One batched engine, one correlator pass per sample step
+    and wave number."""
+    systems = make_systems(settings, n_per_replica, dt, seed)
+    pos = relaxed_start(systems, seed, relax_steps)
+    e = B.Engine(systems, ni_start=-trans_steps)
+    e.set_positions(pos)
+    e.run(trans_steps)
+    tw_steps = sorted(set(int(t) for t in t_ws))
+    e.reserve_snapshots(len(tw_steps))
+    events = {}
+    for k, tw in enumerate(tw_steps):
+        for l in lags:
+            events.setdefault(tw + int(l), []).append((k, int(l)))
+    stops = sorted(set(events) | set(tw_steps))
+    nbins = int(round(G_BINS * G_RANGE[1] / (G_RANGE[1] - G_RANGE[0])))
+    rows_x, rows_y = [], []
+    ni = 0
+    for stop in stops:
+        if stop > ni:
+            e.run(stop - ni)
+            ni = stop
+        if stop in tw_steps:
+            e.snapshot(tw_steps.index(stop))
+        if stop not in events:
+            continue
+        slots = [k for k, _ in events[stop]]
+        gf = g_features(e.gder(nbins, G_RANGE[1]), systems)
+        for q in ks:
+            c = e.correlate(slots, float(q))
+            for j, (k, lag) in enumerate(events[stop]):
+                tw_t, lag_t = max(tw_steps[k], 1) * dt, lag * dt
+                for r, (phi, tfin) in enumerate(settings):
+                    msd = max(float(c[j, r]["msd_big"]), 1e-12)
+                    rows_x.append([phi, tfin, math.log10(tw_t), math.log10(lag_t), q])
+                    rows_y.append(np.concatenate([[c[j, r]["fself_big"], math.log10(msd)], gf[r]]))
+    e.close()
+    return np.array(rows_x, np.float32), np.array(rows_y, np.float32)
+
+
+# ------------------------------------------------------------------ model
+@dataclasses.dataclass
+class Scaler:
+    mean: np.ndarray
+    std: np.ndarray
+
+    @classmethod
+    def fit(cls, a):
+        s = a.std(0)
+        return cls(a.mean(0), np.where(s > 1e-8, s, 1.0))
+
+    def fwd(self, a):
+        return ((a - self.mean) / self.std).astype(np.float32)
+
+    def inv(self, a):
+        return a * self.std + self.mean
+
+
+class SurrogateModel:
+    """Normalisation + the GPU network."""
+
+    def __init__(self, width=256, depth=4, batch=4096, seed=1):
+        self.net = B.Surrogate(n_in=5, n_out=N_OUT, width=width, depth=depth, batch=batch, seed=seed)
+        self.sx = self.sy = None
+
+    def fit(self, X, Y, steps=2000, lr=1e-3):
+        if self.sx is None:
+            self.sx, self.sy = Scaler.fit(X), Scaler.fit(Y)
+        self.net.set_data(self.sx.fwd(X), self.sy.fwd(Y))
+        return self.net.train(steps, lr)
+
+    def predict(self, X):
+        return self.sy.inv(self.net.predict(self.sx.fwd(np.asarray(X, np.float32))))
+
+    def close(self):
+        self.net.close()
+
+
+# ------------------------------------------------------------------ proposals
+def crossing(ts, fs, target):
+    """Linear interpolation of the first crossing of fs(ts) through target
+    (fs decreasing in ts); nearest end when there is none."""
+    ts, fs = np.asarray(ts, np.float64), np.asarray(fs, np.float64)
+    o = np.argsort(ts)
+    ts, fs = ts[o], fs[o]
+    for i in range(len(ts) - 1):
+        a, b = fs[i] - target, fs[i + 1] - target
+        if a == 0:
+            return float(ts[i])
+        if a * b < 0:
+            return float(ts[i] + (ts[i + 1] - ts[i]) * a / (a - b))
+    return float(ts[np.argmin(np.abs(fs - target))])
+
+
+def propose_temperature(model, phi, log_tw, log_t, k, target=0.5, t_range=(0.05, 1.0), grid=400):
+    """Quench temperature at which the surrogate puts F_s = target."""
+    ts = np.linspace(t_range[0], t_range[1], grid)
+    X = np.stack([np.full(grid, phi), ts, np.full(grid, log_tw), np.full(grid, log_t), np.full(grid, k)], 1)
+    fs = model.predict(X)[:, 0]
+    return crossing(ts, -fs, -target)  # F_s decreases as T rises
+
+
+def fs_at(settings, tw, lag, k, seeds, n_per_replica=1000, dt=1e-4):
+    """Plain simulation (the judge): F_s(k; t_w, t_w + lag) per setting,
+    averaged over seeds, plus the sample rows of the whole run (8 lags up to
+    `lag`, three wave numbers around k) for training."""
+    reps = [s for s in settings for _ in seeds]
+    lags = sorted(set(np.unique(np.geomspace(max(1, lag // 64), lag, 8).astype(int)).tolist()) | {int(lag)})
+    ks = [0.7 * k, k, 1.3 * k]
+    X, Y = simulate(reps, [tw], lags, ks, n_per_replica=n_per_replica, dt=dt, seed=int(seeds[0]))
+    sel = (np.abs(X[:, 3] - math.log10(lag * dt)) < 1e-6) & (np.abs(X[:, 4] - np.float32(k)) < 1e-5)
+    rows = X[sel]
+    fs = np.zeros(len(settings))
+    for i, (phi, tfin) in enumerate(settings):
+        m = np.abs(rows[:, 1] - np.float32(tfin)) < 1e-7
+        fs[i] = Y[sel][m, 0].mean()
+    return fs, X, Y
+
+
+def crossing_study(phi=0.52, tw=100, lag=400, k=7.0, budget=6, seeds=(1, 2, 3, 4), t_range=(0.05, 1.0),
+                   truth_points=24, pretrain=None, fit_steps=1500, n_per_replica=1000, dt=1e-4):
+    """Locate T* with F_s(k; t_w, t_w + lag) = 0.5 with `budget` simulated
+    temperatures, by a uniform grid and by surrogate proposals (half the
+    budget on a coarse grid, the rest proposed one at a time, each simulated
+    and added to the training set).  The truth is a dense plain sweep.
+    Returns a dict of estimates and errors."""
+    log_tw, log_t = math.log10(max(tw, 1) * dt), math.log10(lag * dt)
+    ts_truth = np.linspace(t_range[0], t_range[1], truth_points)
+    f_truth, _, _ = fs_at([(phi, t) for t in ts_truth], tw, lag, k, seeds, n_per_replica, dt)
+    t_star = crossing(ts_truth, f_truth, 0.5)
+    # uniform grid
+    ts_grid = np.linspace(t_range[0], t_range[1], budget)
+    f_grid, _, _ = fs_at([(phi, t) for t in ts_grid], tw, lag, k, seeds, n_per_replica, dt)
+    t_grid = crossing(ts_grid, f_grid, 0.5)
+    # surrogate: coarse grid, then proposals
+    n0 = max(2, budget // 2)
+    ts_s = list(np.linspace(t_range[0], t_range[1], n0))
+    f_s, X, Y = fs_at([(phi, t) for t in ts_s], tw, lag, k, seeds, n_per_replica, dt)
+    f_s = list(f_s)
+    if pretrain is not None:
+        X, Y = np.concatenate([pretrain[0], X]), np.concatenate([pretrain[1], Y])
+    model = SurrogateModel(seed=5)
+    model.fit(X, Y, steps=fit_steps)
+    proposals = []
+    for _ in range(budget - n0):
+        tp = propose_temperature(model, phi, log_tw, log_t, k, 0.5, t_range)
+        tp = float(np.clip(tp, t_range[0], t_range[1]))
+        if min(abs(tp - t) for t in ts_s) < 1e-3:  # already simulated: step to the bracket's midpoint
+            tp = 0.5 * (tp + sorted(ts_s, key=lambda t: abs(t - tp))[1])
+        proposals.append(tp)
+        fp, Xp, Yp = fs_at([(phi, tp)], tw, lag, k, seeds, n_per_replica, dt)
+        ts_s.append(tp)
+        f_s.append(float(fp[0]))
+        X, Y = np.concatenate([X, Xp]), np.concatenate([Y, Yp])
+        model.fit(X, Y, steps=fit_steps // 2)
+    model.close()
+    t_sur = crossing(ts_s, f_s, 0.5)  # the simulations judge: interpolate simulated values
+    return {"t_star": t_star, "grid": t_grid, "surrogate": t_sur, "err_grid": abs(t_grid - t_star),
+            "err_surrogate": abs(t_sur - t_star), "proposals": proposals, "budget": budget}

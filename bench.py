@@ -51,6 +51,10 @@ def parse():
     ap.add_argument("--threads", type=int, default=0, help="CTA size (default: engine's)")
     ap.add_argument("--relax-steps", type=int, default=2000,
                     help="capped-force relaxation steps; 0 starts from a jittered lattice instead")
+    ap.add_argument("--mode", default="plain", choices=["plain", "persistent"],
+                    help="one launch per time step, or persistent cluster launches of many steps")
+    ap.add_argument("--cluster", type=int, default=0, help="CTAs per cluster in persistent mode")
+    ap.add_argument("--autotune", action="store_true", help="time brick shapes during warm-up, keep the fastest")
     return ap.parse_args()
 
 
@@ -251,6 +255,25 @@ def reference_cuda(steps=200):
             "ms_per_step": ms.value / steps}
 
 
+def correlator_leg(eng, P, slots=16, iters=20, q=6.19):
+    """Waiting-time correlator on the bench batch: `slots` displacement
+    snapshots, then all of them reduced against the current state in one
+    call.  Traffic per call: current displacement + every snapshot (FP64 x 3)
+    and the global index, (24 (slots + 1) + 4) bytes per particle."""
+    eng.reserve_snapshots(slots)
+    for k in range(slots):
+        eng.snapshot(k)
+        eng.run(1)
+    sl = list(range(slots))
+    eng.correlate(sl, q)
+    ms = cuda_time(eng, lambda: eng.correlate(sl, q), iters)
+    t = ms / 1e3 / iters
+    traffic = (24 * (slots + 1) + 4) * P
+    return {"slots": slots, "ms_per_call": t * 1e3, "evaluations_per_s": P * slots / t,
+            "unit": "(particle, t_w) evaluations/s", "achieved_gbs": traffic / t / 1e9,
+            "bytes_per_call": traffic, "note": "call time includes the host read-back of the sums"}
+
+
 _RELAXED_CACHE = {}
 
 
@@ -281,11 +304,12 @@ def run_ours(args):
     pos = relaxed_positions(systems, 777 + rank, args.relax_steps)
     P = sum(s.n for s in systems)
     S = args.md_steps
-    eng = B.Engine(systems, graph_steps=96, brick=args.brick, threads=args.threads)
+    eng = B.Engine(systems, graph_steps=96, brick=args.brick, threads=args.threads, mode=args.mode,
+                   cluster=args.cluster, autotune=int(args.autotune))
     eng.set_positions(pos)
-    info = eng.info()
     for _ in range(args.warmup):
         eng.run(S)
+    info = eng.info()  # after warm-up: the autotuner may have changed the layout
     clocks = ClockSampler(local)
     clocks.start()
     if dist:
@@ -310,8 +334,10 @@ def run_ours(args):
             "data": "synthetic: uniform random positions relaxed by 2000 capped-force steps (GPU)",
             "config": dict(desc, md_steps_per_bench_step=S, mobility="reference 1/sigma",
                            l2="inputs larger than L2" if P * 112 > 126e6 else "state fits in L2",
-                           brick=list(info.brick), threads=info.threads, cell_capacity=info.cell_capacity),
-            "gpu_launches": int(launches + args.steps * math.ceil(S / 96)),
+                           brick=list(info.brick), threads=info.threads, cell_capacity=info.cell_capacity,
+                           mode=args.mode, cluster=info.cluster if args.mode == "persistent" else None,
+                           autotune=bool(args.autotune)),
+            "gpu_launches": int(args.steps * (math.ceil(S / 96) + (S if args.mode == "plain" else math.ceil(S / 96)))),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "alg_bytes_per_launch": ALG_BYTES_PER_PARTICLE_STEP * P,
@@ -348,6 +374,7 @@ def run_ours(args):
         except Exception as ex:  # reported, never fatal for the bench line
             line["reference_cuda"] = {"error": str(ex)[:200]}
         line["cpu_baseline"] = cpu_baseline()
+        line["correlator"] = correlator_leg(eng, P)
     eng.close()
     if dist:
         dist.destroy_process_group()

@@ -212,6 +212,9 @@ typedef struct bd_engine bd_engine;
                              seed, small with seed+1, subsequence = index within
                              the species (main.cu:478-484) */
 #define BD_RNG_NOISE 2    /* caller-supplied N(0,1) values (bd_engine_set_noise) */
+#define BD_RNG_RANNEW64 3 /* one rannew64 stream per particle (rannew64.cu:55-126),
+                             idum = seed + particle index, 4 uniforms per step,
+                             Box-Muller in float; 2008 bytes of state per particle */
 
 #define BD_MODE_AUTO 0
 #define BD_MODE_PLAIN 1       /* one launch per step, steps captured in CUDA graphs */
@@ -286,11 +289,47 @@ int bd_engine_get_positions(bd_engine *e, float *pos_host, float *raw_host);
 /* g(r) counts of the current state: counts_host[nsys][4][nbins] (bb, bs, sb,
  * ss ordered pairs, get_gder.cu arithmetic), exact integers. */
 int bd_engine_gder(bd_engine *e, int nbins, float range, unsigned long long *counts_host);
+#define BD_GDER_AUTO 0       /* per replica: cell-bounded when the range is small against the box */
+#define BD_GDER_ALL_PAIRS 1  /* every pair, as get_gder_dev (get_gder.cu:69-127) */
+#define BD_GDER_CELLS 2      /* only cells within the range (BD_ERR_ARG if a replica's box
+                                is under 4 + 2 ceil(range / cell side) cells) */
+/* bd_engine_gder with an explicit candidate search; every method gives the
+ * same exact counts. */
+int bd_engine_gder_method(bd_engine *e, int nbins, float range, int method, unsigned long long *counts_host);
 /* BD_RNG_NOISE: N(0,1) values for the next step, 3 per particle (set_positions order). */
 int bd_engine_set_noise(bd_engine *e, const float *noise_host);
 /* Interacting partners of every particle and a hash of their indices (the
  * neighbour set), from the engine's own pair selection.  Host outputs. */
 int bd_engine_census(bd_engine *e, int *nbr_count, unsigned long long *nbr_hash);
+
+/* ---- waiting-time correlations ---------------------------------------------
+ * The reference measures F_s(q; t_w, t_w + tau) and the MSD at a waiting time
+ * t_w by restarting from the configuration written at t_w (main.cu:809-835,
+ * run-fself.sh:149-197) and evaluating fself_isotropic (fself.cu:3-21) and
+ * the MSD loop (main.cu:776-797) against the restart origin (main.cu:497-506).
+ * The engine keeps the FP64 displacement of every particle at each t_w in a
+ * snapshot slot (24 bytes per particle per slot) and reduces all requested
+ * (slot, replica) pairs in one pass. */
+typedef struct bd_correlation {
+    long long lag_steps;         /* steps since the snapshot */
+    double fself_big, fself_sml; /* (1/N_s) sum sin(q|dr|) / (q|dr|), FP64 */
+    double msd_big, msd_sml;     /* (1/N_s) sum |dr|^2 */
+    double r4_big, r4_sml;       /* (1/N_s) sum |dr|^4 (non-Gaussian parameter) */
+} bd_correlation;
+
+/* Room for nslots snapshots (keeps those already taken). */
+int bd_engine_reserve_snapshots(bd_engine *e, int nslots);
+/* Record the current displacement of every particle in `slot`.  Taken just
+ * before the reference's origin step (next step index 0) it is that origin. */
+int bd_engine_snapshot(bd_engine *e, int slot);
+/* Correlations of the current state with slots[0..nslots) (at most 64):
+ * out[j * nsys + r] for slot j, replica r.  BD_ERR_STATE if a slot is empty,
+ * predates bd_engine_set_positions, or predates the origin step. */
+int bd_engine_correlate(bd_engine *e, const int *slots, int nslots, double q, bd_correlation *out);
+/* FP64 displacement of every particle since the origin step (or since
+ * bd_engine_set_positions before it), float3-like triples in the
+ * set_positions order: the reference's rr_raw - rr_ini (main.cu:776-797). */
+int bd_engine_get_displacements(bd_engine *e, double *dsp_host);
 
 #ifdef __cplusplus
 }

@@ -341,6 +341,29 @@ double or_rannew64_next(or_rannew64_state *s) {
     return omm * ((double)uu);
 }
 
+/* Gaussians of the engine's per-particle rannew64 mode: particle p uses
+ * rannew64 seeded with idum = seed + p; each step takes 4 uniforms (double,
+ * narrowed to float) and applies Box-Muller on (u0, u1) -> x, y and
+ * (u2, u3) -> z.  noise[(s * n + p) * 3 + k]. */
+void or_rannew64_particle_noise(long long seed, int n, int steps, float *noise) {
+    or_rannew64_state st;
+    for (int p = 0; p < n; p++) {
+        or_rannew64_seed(&st, (long)(seed + p));
+        for (int s = 0; s < steps; s++) {
+            float u[4];
+            for (int k = 0; k < 4; k++) u[k] = (float)or_rannew64_next(&st);
+            const float tiny = 1.17549435e-38f;
+            float r0 = sqrtf(-2.0f * logf(u[0] > tiny ? u[0] : tiny));
+            float r1 = sqrtf(-2.0f * logf(u[2] > tiny ? u[2] : tiny));
+            float t0 = 6.2831853f * u[1], t1 = 6.2831853f * u[3];
+            float *o = noise + ((size_t)s * n + p) * 3;
+            o[0] = r0 * cosf(t0);
+            o[1] = r0 * sinf(t0);
+            o[2] = r1 * cosf(t1);
+        }
+    }
+}
+
 /* Contracting_Vector3D::add_statistics, Contracting_Vector3D.cu:57-164, float
  * arithmetic; the periodic image uses floor() of the double sum
  * side_inv*d + 0.5 (Contracting_Vector3D.cu:101-105). */

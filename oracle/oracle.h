@@ -49,6 +49,7 @@ int or_ref_sampling_indexes(float minimal_decade, float run_time, float dt, int 
 /* reference rannew64 (rannew64.cu:55-126) with explicit state (one stream) */
 typedef struct { uint64_t useed[250]; uint64_t uuy; int np, nq, init; } or_rannew64_state;
 void or_rannew64_seed(or_rannew64_state *s, long idum);
+void or_rannew64_particle_noise(long long seed, int n, int steps, float *noise);
 double or_rannew64_next(or_rannew64_state *s);
 /* Contracting_Vector3D::add_statistics (Contracting_Vector3D.cu:57-164) in the
  * reference's float arithmetic; ata: 3 x bins x bins, atb: 3 x bins. side<=0:

@@ -80,6 +80,7 @@ def oracle_lib():
         L.or_ref_sampling_indexes.argtypes = [C.c_float, C.c_float, C.c_float, C.c_int, _i32p, C.c_int]
         L.or_ref_sampling_indexes.restype = C.c_int
         L.or_rannew64_next.restype = C.c_double
+        L.or_rannew64_particle_noise.argtypes = [C.c_longlong, C.c_int, C.c_int, _f32p]
         L.or_ref_cv3d_add.argtypes = [C.c_int, C.c_float, _f32p, _f32p, C.c_int, C.c_float, _f32p, _f32p]
         L.or_ref_cv3d_add.restype = C.c_int
         L.or_philox4x32_10.argtypes = [_u32p, _u32p, _u32p]
@@ -93,6 +94,13 @@ def oracle_lib():
         L.or_eng_fself_msd.argtypes = [C.c_int, _f64p, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         _oracle = L
     return _oracle
+
+
+def rannew64_particle_noise(seed: int, n: int, steps: int) -> np.ndarray:
+    """N(0,1) noise [steps, n, 3] of the engine's per-particle rannew64 mode."""
+    out = np.zeros((steps, n, 3), np.float32)
+    oracle_lib().or_rannew64_particle_noise(int(seed), int(n), int(steps), out)
+    return out
 
 
 def ref_available() -> bool:

@@ -152,3 +152,40 @@ def test_graph_relaunch_after_single_steps():
     for _ in range(402):
         e2.run(1)
     np.testing.assert_array_equal(e1.get_positions()[0], e2.get_positions()[0])
+
+
+def _ragged(n=6, seed=40):
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        nb = int(rng.integers(100, 900))
+        ns = int(rng.integers(100, 900))
+        out.append(system(nb, ns, float(rng.uniform(0.45, 0.56)), seed + k, T0=float(rng.uniform(0.1, 1.0))))
+    return zip(*out)
+
+
+def test_persistent_cluster_mode_bit_identical_to_plain():
+    systems, poss = _ragged()
+    pos = np.concatenate(poss)
+    ep = B.Engine(list(systems), mode="persistent", cluster=4)
+    ep.set_positions(pos)
+    ep.run(96 + 40)  # one persistent graph chunk + one direct persistent launch
+    ep.run(77)
+    e1 = B.Engine(list(systems))
+    e1.set_positions(pos)
+    e1.run(213)
+    np.testing.assert_array_equal(ep.get_positions()[0], e1.get_positions()[0])
+    np.testing.assert_array_equal(ep.get_positions()[1], e1.get_positions()[1])
+
+
+def test_autotuner_changes_speed_not_results():
+    systems, poss = _ragged(4, 70)
+    pos = np.concatenate(poss)
+    for mode in ("plain", "persistent"):
+        ea = B.Engine(list(systems), mode=mode, autotune=1)
+        ea.set_positions(pos)
+        ea.run(300)
+        e1 = B.Engine(list(systems))
+        e1.set_positions(pos)
+        e1.run(300)
+        np.testing.assert_array_equal(ea.get_positions()[0], e1.get_positions()[0])
