@@ -43,7 +43,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="aging", choices=["aging", "batched", "large", "small"])
+    ap.add_argument("--workload", default="aging", choices=["aging", "batched", "large", "small", "surrogate"],
+                    help="surrogate: training throughput of the learned surrogate only")
     ap.add_argument("--replicas", type=int, default=64)
     ap.add_argument("--md-steps", type=int, default=960)
     ap.add_argument("--no-extras", action="store_true", help="skip plain/e2e/reference-CUDA/CPU legs")
@@ -274,6 +275,46 @@ def correlator_leg(eng, P, slots=16, iters=20, q=6.19):
             "bytes_per_call": traffic, "note": "call time includes the host read-back of the sums"}
 
 
+SURROGATE_SIZES = [(256, 5)] + [(256, 256)] * 3 + [(34, 256)]       # live (N, K) per layer
+SURROGATE_PADDED = [(256, 64)] + [(256, 256)] * 3 + [(128, 256)]    # as executed (K and N padded)
+
+
+def surrogate_flops(sizes, batch):
+    """Forward, weight-gradient and input-gradient GEMM FLOPs of one training step."""
+    fwd = sum(2 * batch * n * k for n, k in sizes)
+    dx = sum(2 * batch * n * k for n, k in sizes[1:])
+    return 2 * fwd + dx
+
+
+def surrogate_leg(steps=200, warmup=20, batch=4096):
+    """Training steps of the surrogate (5 -> 256 x 4 -> 34, GELU, batch 4096,
+    Adam) on a synthetic 1e5-sample set, each step one CUDA graph of
+    gather, 5 forward GEMMs, 5 weight-gradient and 4 input-gradient GEMMs,
+    bias gradients and Adam."""
+    from bd_aging_b200 import lib as B
+    import torch
+    rng = np.random.default_rng(0)
+    x = rng.uniform(-1, 1, (100000, 5)).astype(np.float32)
+    y = np.tanh(x @ rng.normal(size=(5, 34))).astype(np.float32)
+    s = B.Surrogate(batch=batch, seed=1)
+    s.set_data(x, y)
+    s.train(warmup)
+    st = torch.cuda.ExternalStream(s.stream_handle())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    loss = s.train(steps)
+    e1.record(st)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    s.close()
+    useful, executed = surrogate_flops(SURROGATE_SIZES, batch), surrogate_flops(SURROGATE_PADDED, batch)
+    return {"ms_per_train_step": ms, "useful_tflops": useful / (ms / 1e3) / 1e12,
+            "executed_tflops": executed / (ms / 1e3) / 1e12, "gflop_per_step_useful": useful / 1e9,
+            "gflop_per_step_executed": executed / 1e9, "batch": batch, "final_loss": loss,
+            "gemm_launches_per_step": 14}
+
+
 _RELAXED_CACHE = {}
 
 
@@ -288,7 +329,28 @@ def relaxed_positions_single(nb, ns, side):
     return _RELAXED_CACHE[key]
 
 
+def run_surrogate_only(args):
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    r = surrogate_leg(steps=max(1, args.steps) * 20, warmup=max(3, args.warmup))
+    peak = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak = json.load(f).get("bf16_tflops")
+    except (OSError, ValueError):
+        pass
+    print(json.dumps({"metric": "surrogate training throughput", "value": r["useful_tflops"], "unit": "TFLOP/s",
+                      "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                      "dtype": "bf16 x bf16 -> f32", "data": "synthetic 1e5 x (5 -> 34)",
+                      "config": {"workload": "MLP 5->256x4->34 GELU, batch 4096, Adam"},
+                      "roofline": {"bound": "tensor", "achieved": r["executed_tflops"], "peak": peak,
+                                   "unit": "TFLOP/s", "frac": (r["executed_tflops"] / peak) if peak else None},
+                      "surrogate": r}))
+
+
 def run_ours(args):
+    if args.workload == "surrogate":
+        return run_surrogate_only(args)
     import torch
     from bd_aging_b200 import lib as B
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -375,6 +437,8 @@ def run_ours(args):
             line["reference_cuda"] = {"error": str(ex)[:200]}
         line["cpu_baseline"] = cpu_baseline()
         line["correlator"] = correlator_leg(eng, P)
+        eng.close()
+        line["surrogate"] = surrogate_leg()
     eng.close()
     if dist:
         dist.destroy_process_group()
