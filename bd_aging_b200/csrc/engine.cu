@@ -204,6 +204,8 @@ int configure_kernels(bd_engine *e) {
     BD_ATTR(kRngNoise)
     BD_ATTR(kRngRannew64)
 #undef BD_ATTR
+    if (cudaFuncSetAttribute(k_list_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e->smem) != cudaSuccess)
+        rc = 1;
     return rc ? BD_ERR_CUDA : BD_OK;
 }
 
@@ -222,8 +224,97 @@ int launch_step(bd_engine *e, const StepArgs &a, int ni_off, bool obs, bool cens
     return launch_step_rng<false, false>(e, a, ni_off);
 }
 
+// ---- neighbour-list mode
+ListArgs make_largs(bd_engine *e, int cur) {
+    ListArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.sys = e->d_sys;
+    a.rep_of_sid = e->rep_of_sid;
+    a.gid_of = e->gid_of;
+    a.np = (int)e->P;
+    a.pos_in = e->lpos[cur & 1];
+    a.pos_out = e->lpos[(cur + 1) & 1];
+    a.lo_x = e->lo[0]; a.lo_y = e->lo[1]; a.lo_z = e->lo[2];
+    a.dsp_x = e->dsp[0]; a.dsp_y = e->dsp[1]; a.dsp_z = e->dsp[2];
+    a.nbr = e->nbr;
+    a.nnb = e->nnb;
+    a.pbuild = e->pbuild;
+    a.flag = e->lflag;
+    a.nrep = e->R;
+    a.x0 = e->x0;
+    a.curand_states = e->cr;
+    a.noise = e->noise;
+    a.rn_ring = e->rn_ring;
+    a.rn_lcg = e->rn_lcg;
+    a.rn_ni0 = e->rn_ni0;
+    a.status = e->status;
+    a.ni_first = e->ni_first;
+    a.rng_stream = e->rng_stream;
+    a.nbr_count = e->nbr_count;
+    a.nbr_hash = e->nbr_hash;
+    return a;
+}
+int rebuild_grid(bd_engine *e, long long work) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->dev);
+    return (int)std::max(1LL, std::min(work, (long long)sms * 4));
+}
+// Cell buckets (buffer 0) from the by-id positions of phase `cur`: `any`
+// gates the work, `rflag` (per replica, or null for all) selects replicas
+// (e->lflag inside steps; e->d_one and null for observation passes).
+int list_bin(bd_engine *e, int cur, const int *any, const int *rflag) {
+    k_list_clear<<<rebuild_grid(e, div_up(e->C, 256)), 256, 0, e->stream>>>(e->cnt[0], e->C, any);
+    k_list_bin<<<rebuild_grid(e, div_up(e->P, 256)), 256, 0, e->stream>>>(e->lpos[cur & 1], (int)e->P, e->rep_of_sid,
+                                                                        e->d_sys, e->cnt[0], e->pos[0], e->cap,
+                                                                        e->status, any, rflag);
+    BD_LAUNCH_CHECK();
+    return BD_OK;
+}
+// Rebuild the lists of the flagged replicas (every kernel exits at once when
+// no replica is flagged).  Rebuild decisions are per replica, so a replica
+// gets the same lists alone as in any batch.
+int list_rebuild(bd_engine *e, int cur) {
+    int rc = list_bin(e, cur, e->lflag + e->R, e->lflag);
+    if (rc) return rc;
+    ListBuild lb{e->nbr, e->nnb, e->pbuild, e->lpos[cur & 1], e->lflag, e->R};
+    k_list_build<<<rebuild_grid(e, e->nbricks), e->threads, e->smem, e->stream>>>(make_args(e, 0, 0), lb);
+    k_list_done<<<1, 256, 0, e->stream>>>(e->lflag, e->R, e->d_builds);
+    BD_LAUNCH_CHECK();
+    return BD_OK;
+}
+template <int RNG>
+int launch_list_step_t(bd_engine *e, const ListArgs &a, int ni_off) {
+    k_step_list<RNG><<<div_up(e->P, 256), 256, 0, e->stream>>>(a, e->d_ni, ni_off);
+    BD_LAUNCH_CHECK();
+    return BD_OK;
+}
+// one list-mode step in phase `cur`: conditional rebuild, then the step
+int list_step(bd_engine *e, int cur, int ni_off) {
+    int rc = list_rebuild(e, cur);
+    if (rc) return rc;
+    const ListArgs a = make_largs(e, cur);
+    switch (e->rng) {
+        case BD_RNG_CURAND: return launch_list_step_t<kRngCurand>(e, a, ni_off);
+        case BD_RNG_RANNEW64: return launch_list_step_t<kRngRannew64>(e, a, ni_off);
+        default: return launch_list_step_t<kRngPhilox>(e, a, ni_off);
+    }
+}
+// observation passes read cell buckets: rebuild them from the by-id positions
+int sync_buckets(bd_engine *e) { return e->list ? list_bin(e, e->cur, e->d_one, nullptr) : BD_OK; }
+
 // k steps outside graphs (k = 1 in plain mode): launch, advance the counter
 int direct_steps(bd_engine *e, int k) {
+    if (e->list) {
+        for (int i = 0; i < k; i++) {
+            int rc = list_step(e, e->cur + i, i);
+            if (rc) return rc;
+        }
+        k_advance_counter<<<1, 1, 0, e->stream>>>(e->d_ni, k);
+        BD_LAUNCH_CHECK();
+        e->cur = (e->cur + k) & 1;
+        e->ni += k;
+        return BD_OK;
+    }
     StepArgs a = make_args(e, e->cur, 1);
     int rc = e->mode == BD_MODE_PERSISTENT ? launch_persistent(e, a, k) : launch_step(e, a, 0, false, false);
     if (rc) return rc;
@@ -241,7 +332,9 @@ int build_graph(bd_engine *e) {
     cudaGraph_t g;
     BD_CUDA_TRY(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
     int rc = BD_OK;
-    if (e->mode == BD_MODE_PERSISTENT) {
+    if (e->list) {
+        for (int j = 0; j < e->graph_steps && rc == BD_OK; j++) rc = list_step(e, e->cur + j, j);
+    } else if (e->mode == BD_MODE_PERSISTENT) {
         StepArgs a = make_args(e, e->cur, 1);
         rc = launch_persistent(e, a, e->graph_steps);
     } else {
@@ -266,7 +359,8 @@ void free_engine(bd_engine *e) {
                     e->lo[0], e->lo[1], e->lo[2], e->dsp[0], e->dsp[1], e->dsp[2], e->gid_of, e->rep_of_sid,
                     e->rep_of_gid, e->x0, e->obs, e->snap, e->nbr_count, e->nbr_hash, e->cr, e->noise,
                     e->status, e->d_ni, e->out_pos, e->out_raw, e->d_cl_start, e->d_cl_bricks, e->rn_ring, e->rn_lcg,
-                    e->snaps, e->d_segs, e->d_seg_first, e->corr_part, e->corr_out};
+                    e->snaps, e->d_segs, e->d_seg_first, e->corr_part, e->corr_out, e->lpos[0], e->lpos[1],
+                    e->pbuild, e->nbr, e->nnb, e->lflag, e->d_one, e->d_builds};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -378,7 +472,10 @@ int setup_geometry(bd_engine *e) {
         S.sig[2] = d.sigma_sml;
         for (int k = 0; k < 3; k++) S.cut2[k] = S.sig[k] * S.sig[k];
         float rcmax = std::max(S.sig[0], std::max(S.sig[1], S.sig[2]));
-        int nc = (int)std::floor((double)d.side / ((double)rcmax * (1.0 + 1e-5)));
+        const float skin = e->list ? e->skin : 0.f;  // list builds sweep cut + skin
+        for (int k = 0; k < 3; k++) S.lcut2[k] = (S.sig[k] + skin) * (S.sig[k] + skin);
+        S.skin_half2 = 0.25f * skin * skin;
+        int nc = (int)std::floor((double)d.side / ((double)(rcmax + skin) * (1.0 + 1e-5)));
         if (nc < 3) return BD_ERR_ARG;  // box too small for a 27-cell sweep
         S.ncell = nc;
         S.cinv = (float)nc / d.side;
@@ -415,6 +512,7 @@ void bd_engine_opts_default(bd_engine_opts *o) {
     o->cluster = 8;
     o->graph_steps = 96;
     o->qmax = 6.2831853f;
+    o->neighbor_skin = 0.25f;
 }
 
 int bd_engine_create(const bd_system_desc *systems, int nsys, const bd_engine_opts *opts_in, bd_engine **out) {
@@ -429,7 +527,9 @@ int bd_engine_create(const bd_system_desc *systems, int nsys, const bd_engine_op
     e->desc.assign(systems, systems + nsys);
     e->rng = opts.rng;
     if (e->rng < BD_RNG_PHILOX || e->rng > BD_RNG_RANNEW64) { delete e; return BD_ERR_ARG; }
-    e->cap = opts.cell_capacity > 0 ? opts.cell_capacity : 16;
+    // list mode's cells are sized for cut + skin and hold about 1.7x more particles
+    const bool want_list = opts.neighbor_skin > 0.f && opts.mode != BD_MODE_PERSISTENT && opts.rng != BD_RNG_NOISE;
+    e->cap = opts.cell_capacity > 0 ? opts.cell_capacity : (want_list ? 24 : 16);
     if (e->cap > kQueue / 3) { delete e; return BD_ERR_ARG; }  // a row of 3 cells must fit one queue
     if (opts.brick[0] > 0 && opts.brick[1] > 0 && opts.brick[2] > 0) {
         e->bx = opts.brick[0]; e->by = opts.brick[1]; e->bz = opts.brick[2];
@@ -443,7 +543,18 @@ int bd_engine_create(const bd_system_desc *systems, int nsys, const bd_engine_op
     e->ni = e->ni_first = opts.ni_start;
     e->rng_stream = opts.rng_stream;
     e->autotune = opts.autotune;
+    if (!(opts.neighbor_skin >= 0.f) || opts.neighbor_skin > 1.0f) { delete e; return BD_ERR_ARG; }
+    // lists serve plain mode with generated noise; a box too small for the
+    // enlarged cells keeps the sweep
+    e->list = opts.neighbor_skin > 0.f && e->mode == BD_MODE_PLAIN && e->rng != BD_RNG_NOISE;
+    e->skin = e->list ? opts.neighbor_skin : 0.f;
+    if (e->list) e->graph_steps = ((e->graph_steps + 5) / 6) * 6;  // keeps both buffer rotations in phase
     int rc = setup_geometry(e);
+    if (rc == BD_ERR_ARG && e->list) {
+        e->list = false;
+        e->skin = 0.f;
+        rc = setup_geometry(e);
+    }
     if (rc) { delete e; return rc; }
 #define ALLOC(ptr, bytes)                                                    \
     do {                                                                     \
@@ -475,6 +586,19 @@ int bd_engine_create(const bd_system_desc *systems, int nsys, const bd_engine_op
     if (e->rng == BD_RNG_RANNEW64) {
         ALLOC(e->rn_ring, sizeof(unsigned long long) * kRnWords * P);
         ALLOC(e->rn_lcg, sizeof(unsigned long long) * P);
+    }
+    if (e->list) {
+        ALLOC(e->lpos[0], sizeof(float4) * P);
+        ALLOC(e->lpos[1], sizeof(float4) * P);
+        ALLOC(e->pbuild, sizeof(float4) * P);
+        ALLOC(e->nbr, sizeof(int) * (size_t)kMaxNbr * P);
+        ALLOC(e->nnb, sizeof(int) * P);
+        ALLOC(e->lflag, sizeof(int) * (e->R + 1));
+        ALLOC(e->d_one, sizeof(int));
+        ALLOC(e->d_builds, sizeof(long long));
+        cudaMemsetAsync(e->d_builds, 0, sizeof(long long), e->stream);
+        const int one = 1;
+        cudaMemcpyAsync(e->d_one, &one, sizeof(int), cudaMemcpyHostToDevice, e->stream);
     }
 #undef ALLOC
     cudaMemcpyAsync(e->d_sys, e->sysh.data(), sizeof(SysDev) * e->R, cudaMemcpyHostToDevice, e->stream);
@@ -527,6 +651,12 @@ int bd_engine_get_info(const bd_engine *e, bd_engine_info *info) {
     info->cluster = e->cluster;
     info->smem_bytes = e->smem;
     info->next_step = e->ni;
+    info->neighbor_skin = e->list ? e->skin : 0.f;
+    if (e->list) {
+        BD_CUDA_TRY(cudaMemcpyAsync(&info->list_builds, e->d_builds, sizeof(long long), cudaMemcpyDeviceToHost,
+                                    e->stream));
+        BD_CUDA_TRY(cudaStreamSynchronize(e->stream));
+    }
     return BD_OK;
 }
 
@@ -600,7 +730,12 @@ int bd_engine_set_positions(bd_engine *e, const float *pos) {
             if (e->gexec[g]) { cudaGraphExecDestroy(e->gexec[g]); e->gexec[g] = nullptr; }
     }
     k_load<<<div_up((long)P, 256), 256, 0, e->stream>>>(d_staged, (int)P, e->rep_of_sid, e->d_sys, e->cnt[0],
-                                                        e->pos[0], e->cap, e->x0, e->gid_of, e->status);
+                                                        e->pos[0], e->cap, e->x0, e->gid_of, e->status,
+                                                        e->list ? e->lpos[0] : nullptr);
+    if (e->list) {  // every replica's lists are built before its first step
+        std::vector<int> ones(e->R + 1, 1);
+        cudaMemcpyAsync(e->lflag, ones.data(), sizeof(int) * (e->R + 1), cudaMemcpyHostToDevice, e->stream);
+    }
     if (e->rng == BD_RNG_RANNEW64)
         k_rannew64_seed<<<div_up((long)P, 128), 128, 0, e->stream>>>(e->rn_ring, e->rn_lcg, e->d_sys, e->rep_of_sid,
                                                                      e->gid_of, (int)P);
@@ -632,6 +767,7 @@ int run_direct(bd_engine *e, int k) {
 // takes are real steps of the run; results do not depend on the layout
 // (every force sum has a fixed order), only the speed does.
 int autotune_layout(bd_engine *e, long long &nsteps) {
+    if (e->list) return BD_OK;  // list steps do not depend on the brick layout
     struct Cand { int bx, by, bz, t, cl; };
     static const int shapes[][4] = {{4, 4, 3, 128}, {4, 4, 4, 160}, {5, 4, 4, 192}, {4, 3, 3, 96}, {3, 3, 3, 64},
                                     {4, 4, 2, 96},  {2, 2, 2, 64},  {3, 3, 2, 64},  {6, 4, 3, 192}};
@@ -718,7 +854,9 @@ int bd_engine_observe(bd_engine *e, bd_observables *out) {
     if (!e || !out) return BD_ERR_ARG;
     if (!e->loaded) return BD_ERR_STATE;
     BD_CUDA_TRY(cudaMemsetAsync(e->obs, 0, sizeof(double) * kObsCount * e->R, e->stream));
-    StepArgs a = make_args(e, e->cur, 0);
+    int rc0 = sync_buckets(e);
+    if (rc0) return rc0;
+    StepArgs a = make_args(e, obs_buf(e), 0);
     int rc = launch_step(e, a, 0, true, false);
     if (rc) return rc;
     std::vector<double> h((size_t)kObsCount * e->R);
@@ -757,7 +895,11 @@ int bd_engine_get_positions(bd_engine *e, float *pos_host, float *raw_host) {
         if (cudaMalloc(&e->out_pos, sizeof(float) * 3 * P) != cudaSuccess) return BD_ERR_NOMEM;
         if (cudaMalloc(&e->out_raw, sizeof(float) * 3 * P) != cudaSuccess) return BD_ERR_NOMEM;
     }
-    k_export<<<div_up(e->C, 128), 128, 0, e->stream>>>(e->cnt[e->cur], e->pos[e->cur], (int)e->C, e->cap, (int)e->P, e->gid_of,
+    {
+        int rcb = sync_buckets(e);
+        if (rcb) return rcb;
+    }
+    k_export<<<div_up(e->C, 128), 128, 0, e->stream>>>(e->cnt[obs_buf(e)], e->pos[obs_buf(e)], (int)e->C, e->cap, (int)e->P, e->gid_of,
                                                        e->x0, e->dsp[0], e->dsp[1], e->dsp[2], e->out_pos,
                                                        e->out_raw, e->snap);
     BD_LAUNCH_CHECK();
@@ -770,6 +912,7 @@ int bd_engine_gder_method(bd_engine *e, int nbins, float range, int method, unsi
     if (!e || !counts_host || nbins < 1 || nbins > 4096 || !(range > 0)) return BD_ERR_ARG;
     if (method != BD_GDER_AUTO && method != BD_GDER_ALL_PAIRS && method != BD_GDER_CELLS) return BD_ERR_ARG;
     if (!e->loaded) return BD_ERR_STATE;
+    if (int rcb = sync_buckets(e)) return rcb;
     // per replica: cell-bounded when the stencil region is well inside the box
     std::vector<int> m_of(e->R, -1);
     bool any_all = false;
@@ -790,7 +933,7 @@ int bd_engine_gder_method(bd_engine *e, int nbins, float range, int method, unsi
     for (int r = 0; r < e->R; r++) any_all |= m_of[r] < 0;
     cudaError_t le = cudaSuccess;
     if (rc == BD_OK && any_all) {
-        k_export<<<div_up(e->C, 128), 128, 0, e->stream>>>(e->cnt[e->cur], e->pos[e->cur], (int)e->C, e->cap, (int)e->P,
+        k_export<<<div_up(e->C, 128), 128, 0, e->stream>>>(e->cnt[obs_buf(e)], e->pos[obs_buf(e)], (int)e->C, e->cap, (int)e->P,
                                                            e->gid_of, e->x0, e->dsp[0], e->dsp[1], e->dsp[2], nullptr,
                                                            nullptr, e->snap);
         const size_t sm = kGrTile * sizeof(float4) + per * sizeof(unsigned);
@@ -831,11 +974,17 @@ int bd_engine_census(bd_engine *e, int *nbr_count, unsigned long long *nbr_hash)
         if (cudaMalloc(&e->nbr_hash, sizeof(unsigned long long) * e->P) != cudaSuccess) return BD_ERR_NOMEM;
     }
     BD_CUDA_TRY(cudaMemsetAsync(e->obs, 0, sizeof(double) * kObsCount * e->R, e->stream));
-    StepArgs a = make_args(e, e->cur, 0);
-    a.nbr_count = e->nbr_count;
-    a.nbr_hash = e->nbr_hash;
-    int rc = launch_step(e, a, 0, false, true);
-    if (rc) return rc;
+    int rc;
+    if (e->list) {  // from the lists themselves (rebuilt first if they are stale)
+        if ((rc = list_rebuild(e, e->cur))) return rc;
+        k_census_list<<<div_up(e->P, 256), 256, 0, e->stream>>>(make_largs(e, e->cur), e->obs);
+        BD_LAUNCH_CHECK();
+    } else {
+        StepArgs a = make_args(e, e->cur, 0);
+        a.nbr_count = e->nbr_count;
+        a.nbr_hash = e->nbr_hash;
+        if ((rc = launch_step(e, a, 0, false, true))) return rc;
+    }
     BD_CUDA_TRY(cudaMemcpyAsync(nbr_count, e->nbr_count, sizeof(int) * e->P, cudaMemcpyDeviceToHost, e->stream));
     BD_CUDA_TRY(cudaMemcpyAsync(nbr_hash, e->nbr_hash, sizeof(unsigned long long) * e->P, cudaMemcpyDeviceToHost, e->stream));
     return engine_status(e);

@@ -106,6 +106,7 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
 
 }  // namespace bd
 #include "step.cuh"
+#include "nlist.cuh"
 namespace bd {
 
 __global__ void k_advance_counter(long long *ni_base, int k) { *ni_base += k; }
@@ -114,10 +115,11 @@ __global__ void k_advance_counter(long long *ni_base, int k) { *ni_base += k; }
 // Bin particles given in storage order (float4 w = sid | species << 31).
 __global__ void k_load(const float4 *__restrict__ staged, int P, const int *__restrict__ rep_of_sid,
                        const SysDev *sys, int *cnt, float4 *pos, int cap, double *x0, const int *gid_of,
-                       unsigned *st) {
+                       unsigned *st, float4 *pos_sid) {
     int sid = blockIdx.x * blockDim.x + threadIdx.x;
     if (sid >= P) return;
     float4 v = staged[sid];
+    if (pos_sid) pos_sid[sid] = v;  // neighbour-list mode keeps positions by storage id
     const SysDev &S = sys[rep_of_sid[sid]];
     int nc = S.ncell;
     int ix = (int)__fmul_rn(v.x, S.cinv), iy = (int)__fmul_rn(v.y, S.cinv), iz = (int)__fmul_rn(v.z, S.cinv);

@@ -67,6 +67,15 @@ struct bd_engine {
     int nsegs = 0;
     double *corr_part = nullptr, *corr_out = nullptr;
     size_t corr_part_cap = 0, corr_out_cap = 0;
+    // neighbour-list mode (plain mode with generated noise): positions by
+    // storage id (double-buffered, e->cur selects), build positions, lists
+    bool list = false;
+    float skin = 0.f;
+    float4 *lpos[2] = {nullptr, nullptr};
+    float4 *pbuild = nullptr;
+    int *nbr = nullptr, *nnb = nullptr;
+    int *lflag = nullptr, *d_one = nullptr;
+    long long *d_builds = nullptr;  // list builds so far
 };
 
 
@@ -78,6 +87,10 @@ namespace bd {
 int gder_cell_reach(const SysDev &S, float range);
 int launch_gder_cells(bd_engine *e, std::vector<int> &m_of, int nbins, float range,
                       unsigned long long *d_counts);
+
+// cell-bucket buffer holding the current state (list mode rebuilds buffer 0
+// before every observation pass)
+inline int obs_buf(const bd_engine *e) { return e->list ? 0 : e->cur; }
 
 inline int engine_status(bd_engine *e) {
     unsigned bits = 0;

@@ -26,8 +26,8 @@ namespace bd {
 
 constexpr int kGrBrick = 4;
 constexpr int kGrThreads = 256;
-constexpr int kGrTileCells = 128;
-constexpr int kGrMaxCap = 16;
+constexpr int kGrTileCells = 96;
+constexpr int kGrMaxCap = 24;
 constexpr int kGrHomeMax = kGrBrick * kGrBrick * kGrBrick * kGrMaxCap;
 constexpr int kGrTileMax = kGrTileCells * kGrMaxCap;
 constexpr double kGrTol = 1e-3;  // allowed stick-out of a particle from its cell, in cell sides
@@ -271,8 +271,8 @@ int launch_gder_cells(bd_engine *e, std::vector<int> &m_of, int nbins, float ran
     if (ce == cudaSuccess) {
         GrArgs a;
         a.sys = e->d_sys;
-        a.cnt = e->cnt[e->cur];
-        a.pos = e->pos[e->cur];
+        a.cnt = e->cnt[obs_buf(e)];
+        a.pos = e->pos[obs_buf(e)];
         a.bricks = d_bricks;
         a.cap = e->cap;
         a.nbins = nbins;

@@ -22,7 +22,7 @@
 
 namespace bd {
 
-constexpr int kQueue = 48;            // queue length per thread; >= one row (3 cells x 16 slots)
+constexpr int kQueue = 72;            // queue length per thread; >= one row (3 cells x 24 slots)
 constexpr unsigned kNoShift = 0x15u;  // shift code of a halo cell that did not wrap
 
 typedef unsigned long long f2;  // two floats in one 64-bit register (lo, hi)
@@ -197,28 +197,20 @@ __device__ __forceinline__ void sweep_row(const BrickSmem &sm, const float *view
     }
 }
 
-template <int RNG, bool OBS, bool CENSUS>
-__device__ void process_brick(const StepArgs &a, int bidx, long long ni, unsigned char *smem_raw) {
-    const int4 br = a.bricks[bidx];
-    const SysDev &S = a.sys[br.x];
+// Stage the cells of brick `br` plus a one-cell halo into shared memory
+// (steps 1-2 above) with the squared cut distances c2bb, c2bs, c2ss in the
+// per-home-species views.  Returns false (status set) when the staging
+// capacity is exceeded.  On return the block is synchronised and sm.start /
+// sm.hstart hold the staged and home prefixes (totals M, MH at [nh]).
+__device__ __forceinline__ bool stage_brick(const StepArgs &a, const int4 br, const SysDev &S, const BrickSmem &sm,
+                                            float c2bb, float c2bs, float c2ss) {
     const int nc = S.ncell;
     const int ox = br.y, oy = br.z, oz = br.w;
     const int wx = min(a.bx, nc - ox), wy = min(a.by, nc - oy), wz = min(a.bz, nc - oz);
     const int hx = wx + 2, hy = wy + 2, hz = wz + 2, nh = hx * hy * hz;
-    BrickSmem sm;
-    brick_smem_layout((a.bx + 2) * (a.by + 2) * (a.bz + 2), a.smax, blockDim.x, &sm, smem_raw);
     const int tid = threadIdx.x, T = blockDim.x;
     const int vstride = a.smax + 2;
-    const float L = S.L, Linv = S.Linv, cinv = S.cinv;
-    const int cell_base = S.cell_base, part_base = S.part_base;
-    const float c2bb = S.cut2[0], c2bs = S.cut2[1], c2ss = S.cut2[2];
-    const float sgbb = S.sig[0], sgbs = S.sig[1], sgss = S.sig[2];
-
-    if (tid == 0) {
-        const float Tm = step_temperature(S, ni, a.ni_first);
-        sm.amp[0] = amplitude(Tm, S.mob[0], S.dt);
-        sm.amp[1] = amplitude(Tm, S.mob[1], S.dt);
-    }
+    const int cell_base = S.cell_base;
     // 1. halo cells: global index, clamped count, periodic shift code
     for (int h = tid; h < nh; h += T) {
         const int lx = h % hx, ly = (h / hx) % hy, lz = h / (hx * hy);
@@ -239,10 +231,10 @@ __device__ void process_brick(const StepArgs &a, int bidx, long long ni, unsigne
     }
     __syncthreads();
     block_scan2(sm.start, sm.hstart, nh, sm.tmp);
-    const int M = sm.start[nh], MH = sm.hstart[nh];
+    const int M = sm.start[nh];
     if (M > a.smax) {  // staging capacity exceeded: flag and leave the brick
         if (tid == 0) set_status(a.status, kStatCellOverflow);
-        return;
+        return false;
     }
     // 2a. one independent load per staged particle (unsorted)
     for (int t = tid; t < M; t += T) {
@@ -281,6 +273,33 @@ __device__ void process_brick(const StepArgs &a, int bidx, long long ni, unsigne
     }
     __syncthreads();
 
+    return true;
+}
+
+template <int RNG, bool OBS, bool CENSUS>
+__device__ void process_brick(const StepArgs &a, int bidx, long long ni, unsigned char *smem_raw) {
+    const int4 br = a.bricks[bidx];
+    const SysDev &S = a.sys[br.x];
+    const int nc = S.ncell;
+    const int ox = br.y, oy = br.z, oz = br.w;
+    const int wx = min(a.bx, nc - ox), wy = min(a.by, nc - oy), wz = min(a.bz, nc - oz);
+    const int hx = wx + 2, hy = wy + 2, hz = wz + 2, nh = hx * hy * hz;
+    BrickSmem sm;
+    brick_smem_layout((a.bx + 2) * (a.by + 2) * (a.bz + 2), a.smax, blockDim.x, &sm, smem_raw);
+    const int tid = threadIdx.x, T = blockDim.x;
+    const int vstride = a.smax + 2;
+    const float L = S.L, Linv = S.Linv, cinv = S.cinv;
+    const int cell_base = S.cell_base, part_base = S.part_base;
+    const float c2bb = S.cut2[0], c2bs = S.cut2[1], c2ss = S.cut2[2];
+    const float sgbb = S.sig[0], sgbs = S.sig[1], sgss = S.sig[2];
+
+    if (tid == 0) {
+        const float Tm = step_temperature(S, ni, a.ni_first);
+        sm.amp[0] = amplitude(Tm, S.mob[0], S.dt);
+        sm.amp[1] = amplitude(Tm, S.mob[1], S.dt);
+    }
+    if (!stage_brick(a, br, S, sm, c2bb, c2bs, c2ss)) return;
+    const int MH = sm.hstart[nh];
     // 3. forces and update, one thread per home particle
     double acc_pb = 0, acc_ps = 0, acc_v = 0, acc_mb = 0, acc_ms = 0, acc_fs = 0, acc_nb = 0;
     for (int q = tid; q < MH; q += T) {

@@ -105,7 +105,7 @@ __device__ __forceinline__ unsigned long long mix64(unsigned long long x) {
 }
 
 // minibatch rows: x (FP32 [n_data][n_in]) -> X0 [B][k0] and X0^T [k0][B]
-// (BF16, zero padded), targets -> T [B][n_out_pad]
+// (BF16, zero padded), targets -> T [n_out_pad][B]
 __global__ void k_gather(const float *x, const float *y, int n_data, int n_in, int n_out, int k0, int n_out_pad,
                          int B, const int *rows, const long long *step, unsigned long long seed, __nv_bfloat16 *X0,
                          __nv_bfloat16 *X0t, float *T) {
@@ -124,9 +124,9 @@ __global__ void k_gather(const float *x, const float *y, int n_data, int n_in, i
         X0[(size_t)r * k0 + k] = b;
         X0t[(size_t)k * B + r] = b;
     }
-    if (T)
+    if (T)  // targets transposed [n_out_pad][B], as the loss epilogue reads them
         for (int k = threadIdx.x; k < n_out_pad; k += blockDim.x)
-            T[(size_t)r * n_out_pad + k] = (valid && k < n_out) ? y[(size_t)src * n_out + k] : 0.f;
+            T[(size_t)k * B + r] = (valid && k < n_out) ? y[(size_t)src * n_out + k] : 0.f;
 }
 
 // bias gradient: db[n] = sum over the batch of dZ^T[n][:] (fixed order)
@@ -149,29 +149,31 @@ struct AdamArgs {
     const long long *step;  // number of updates so far (incremented by the caller's counter kernel)
 };
 
-// Adam on one weight matrix [N][K] (gradient = sum of the split partials)
-// and its bias; writes the BF16 copies W [N][K] and W^T [K][N].
+// Adam on one weight matrix W [N][K] (gradient = sum of the split partials,
+// stored transposed [splits][K][N] by the weight-gradient GEMM) and its
+// bias; writes the BF16 copies W [N][K] and W^T [K][N].
 __global__ void k_adam(float *w, float *m1, float *m2, const float *part, int splits, int N, int K, int n_live,
                        int k_live, __nv_bfloat16 *wb, __nv_bfloat16 *wbt, AdamArgs a) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // [k][n] order
     if (i >= (size_t)N * K) return;
-    const int n = (int)(i / K), k = (int)(i % K);
+    const int k = (int)(i / N), n = (int)(i % N);
+    const size_t wi = (size_t)n * K + k;
     float gsum = 0.f;
     for (int s = 0; s < splits; s++) gsum += part[(size_t)s * N * K + i];
     const float t = (float)(*a.step + 1);
-    float wv = w[i];
+    float wv = w[wi];
     if (n < n_live && k < k_live) {
-        const float mm = a.b1 * m1[i] + (1.f - a.b1) * gsum;
-        const float vv = a.b2 * m2[i] + (1.f - a.b2) * gsum * gsum;
-        m1[i] = mm;
-        m2[i] = vv;
+        const float mm = a.b1 * m1[wi] + (1.f - a.b1) * gsum;
+        const float vv = a.b2 * m2[wi] + (1.f - a.b2) * gsum * gsum;
+        m1[wi] = mm;
+        m2[wi] = vv;
         const float mh = mm / (1.f - powf(a.b1, t)), vh = vv / (1.f - powf(a.b2, t));
         wv -= a.lr * mh / (sqrtf(vh) + a.eps);
-        w[i] = wv;
+        w[wi] = wv;
     }
     const __nv_bfloat16 b = __float2bfloat16_rn(wv);
-    wb[i] = b;
-    wbt[(size_t)k * N + n] = b;
+    wb[wi] = b;
+    wbt[i] = b;
 }
 __global__ void k_adam_bias(float *b, float *m1, float *m2, const float *g, int N, int n_live, AdamArgs a) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
@@ -210,10 +212,10 @@ struct bd_surrogate {
     std::vector<__nv_bfloat16 *> wb, wbt;
     // activations (BF16 row-major and transposed), pre-activations FP32
     std::vector<__nv_bfloat16 *> h, ht;   // h[0] = input X0; h[l+1] = output of layer l (hidden)
-    std::vector<float *> z;               // z[l] pre-activation of layer l
+    std::vector<float *> z;               // z[l] pre-activation of layer l, transposed [N_l][B]
     std::vector<__nv_bfloat16 *> dz, dzt; // dz[l] gradient w.r.t. z[l]
-    float *y = nullptr, *t = nullptr, *tw = nullptr;  // output [B][Np], target [B][Np], weights [Np]
-    float *part = nullptr;            // split-K partials (largest layer)
+    float *y = nullptr, *t = nullptr, *tw = nullptr;  // output [128][B], target [128][B] (transposed), weights
+    float *part = nullptr;            // weight-gradient split partials [splits][K_l][N_l] per layer
     std::vector<float *> db;          // bias gradients
     float *loss_part = nullptr;
     long long *step = nullptr;
@@ -621,8 +623,8 @@ int bd_surrogate_gradients(bd_surrogate *s, const float *x, const float *y, floa
             cudaMemcpyAsync(hb.data(), s->db[l], s->Np[l] * 4, cudaMemcpyDeviceToHost, s->stream);
             cudaStreamSynchronize(s->stream);
             cudaFree(gsum);
-            for (int nn = 0; nn < s->Nl[l]; nn++)
-                for (int k = 0; k < s->Kl[l]; k++) grad[off++] = hg[(size_t)nn * s->Kp[l] + k];
+            for (int nn = 0; nn < s->Nl[l]; nn++)  // partial sums are [K][N]
+                for (int k = 0; k < s->Kl[l]; k++) grad[off++] = hg[(size_t)k * s->Np[l] + nn];
             for (int nn = 0; nn < s->Nl[l]; nn++) grad[off++] = hb[nn];
         }
         cudaMemcpyAsync(lp.data(), s->loss_part, lp.size() * 4, cudaMemcpyDeviceToHost, s->stream);
@@ -662,8 +664,8 @@ int bd_surrogate_predict(bd_surrogate *s, const float *x, int n, float *y) {
         if (rc) break;
         cudaMemcpyAsync(hy.data(), s->y, hy.size() * 4, cudaMemcpyDeviceToHost, s->stream);
         if (cudaStreamSynchronize(s->stream) != cudaSuccess) rc = BD_ERR_CUDA;
-        for (int i = 0; i < cnt; i++)
-            for (int k = 0; k < s->n_out; k++) y[(size_t)(r0 + i) * s->n_out + k] = hy[(size_t)i * 128 + k];
+        for (int i = 0; i < cnt; i++)  // outputs are [128][B]
+            for (int k = 0; k < s->n_out; k++) y[(size_t)(r0 + i) * s->n_out + k] = hy[(size_t)k * B + i];
     }
     cudaFree(dx);
     cudaFree(drows);
@@ -708,11 +710,14 @@ int bd_umma_gemm_bf16(const unsigned short *a, const unsigned short *b, int M, i
     }
     if (!rc) {
         k_sum_splits<<<div_up((long)M * N, 256), 256, 0, st>>>(part, splits, (size_t)M * N, dc);
-        cudaMemcpyAsync(c, dc, (size_t)M * N * 4, cudaMemcpyDeviceToHost, st);
+        std::vector<float> ct((size_t)M * N);  // the kernel writes C transposed
+        cudaMemcpyAsync(ct.data(), dc, (size_t)M * N * 4, cudaMemcpyDeviceToHost, st);
         unsigned e = 0;
         cudaMemcpyAsync(&e, err, 4, cudaMemcpyDeviceToHost, st);
         if (cudaStreamSynchronize(st) != cudaSuccess) rc = BD_ERR_CUDA;
         else if (e) rc = BD_ERR_TIMEOUT;
+        for (int i = 0; i < M && !rc; i++)
+            for (int j = 0; j < N; j++) c[(size_t)i * N + j] = ct[(size_t)j * M + i];
     }
     cudaFree(da);
     cudaFree(db);

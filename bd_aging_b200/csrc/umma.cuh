@@ -2,13 +2,13 @@
 // surrogate network: C[M][N] = sum_k A[M][k] B[N][k] (both operands
 // K-major, BF16; FP32 accumulation in tensor memory) with fused epilogues.
 //
-// One CTA (4 warps) computes a 128 x 128 tile over a K range of at most 256:
+// One CTA (8 warps) computes a 128 x 128 tile over a K range of at most 256:
 //   * thread 0 issues every TMA load of the range at once (64-wide K chunks,
 //     128-byte swizzle, one mbarrier per chunk, no multicast);
 //   * one lane of warp 1 issues tcgen05.mma (M=128, N=128, K=16) per 16-wide
 //     slice as each chunk lands, then tcgen05.commit to the "done" barrier;
-//   * all four warps read their 32 accumulator rows with tcgen05.ld and apply
-//     the epilogue.
+//   * all eight warps read accumulator rows with tcgen05.ld (warp w: lanes
+//     32 (w % 4) .. + 31, the column half w / 4) and apply the epilogue.
 // Every mbarrier wait is bounded: on expiry the CTA records an error flag,
 // waits (bounded) for its own copies, frees its tensor memory and returns.
 #pragma once
@@ -23,27 +23,29 @@ namespace umma {
 
 constexpr int kBM = 128, kBN = 128, kBK = 64;  // kBK bf16 = one 128-byte swizzle row
 constexpr int kMaxChunks = 4;                   // K range per CTA <= 256
-constexpr int kThreads = 128;
+constexpr int kThreads = 256;  // 8 warps: warp w reads TMEM lanes 32 (w % 4), columns 64 (w / 4)
 constexpr int kStageBytes = kBM * kBK * 2;      // 16 KB per operand tile
 constexpr int kSmemBytes = 2 * kMaxChunks * kStageBytes + 1024 /* align */ + 256 /* barriers */;
 constexpr long kSpinLimit = 1L << 20;
 
 enum Epilogue {
-    kEpiF32 = 0,      // out_f32[z][m][n] = acc (split-K partials)
-    kEpiFwdGelu = 1,  // z = acc + bias: zout, gelu(z) -> out_bf [m][n] and out_bfT [n][m]
-    kEpiFwdOut = 2,   // y = acc + bias -> out_f32; with a target: loss gradient -> out_bf / out_bfT
-    kEpiBwdGelu = 3,  // dz = acc * gelu'(zin) -> out_bf / out_bfT
+    kEpiF32 = 0,      // out_f32[z][n][m] = acc (split-K partials, transposed)
+    kEpiFwdGelu = 1,  // z = acc + bias -> out_f32 [n][m]; gelu(z) -> out_bf [m][n] and out_bfT [n][m]
+    kEpiFwdOut = 2,   // y = acc + bias -> out_f32 [n][m]; with a target [n][m]: loss gradient -> out_bf / out_bfT
+    kEpiBwdGelu = 3,  // dz = acc * gelu'(zin [n][m]) -> out_bf / out_bfT
 };
 
 struct GemmArgs {
     int M, N, K;          // logical sizes (rows of A, rows of B, reduction)
     int k_split;          // K range per blockIdx.z (multiple of 64, <= 256)
     const float *bias;    // [N]
-    float *out_f32;       // kEpiF32: [splits][M][N]; kEpiFwdGelu: z [M][N]; kEpiFwdOut: y [M][N]
+    // FP32 outputs and inputs are stored transposed ([N][M]): the epilogue
+    // thread owns one row m, so consecutive lanes touch consecutive addresses
+    float *out_f32;       // kEpiF32: [splits][N][M]; kEpiFwdGelu: z [N][M]; kEpiFwdOut: y [N][M]
     __nv_bfloat16 *out_bf;   // [M][N]
     __nv_bfloat16 *out_bfT;  // [N][M]
-    const float *zin;     // kEpiBwdGelu: pre-activation [M][N]
-    const float *target;  // kEpiFwdOut: [M][N] or null (inference)
+    const float *zin;     // kEpiBwdGelu: pre-activation [N][M]
+    const float *target;  // kEpiFwdOut: [N][M] or null (inference)
     const float *tweight; // [N] loss weight per output
     int m_valid;          // rows that count in the loss
     int n_valid;          // outputs that count in the loss
@@ -128,6 +130,11 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
+    tmem_ld16(taddr, v);
+    tmem_ld16(taddr + 16, v + 16);
+}
+
 // ----------------------------------------------------------------- math
 __device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678f)); }
 __device__ __forceinline__ float gelu_grad(float z) {
@@ -147,6 +154,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint64_t *done = full + kMaxChunks;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
     __shared__ float red[kThreads / 32];
+    __shared__ float stage[kThreads / 32][32][33];  // per-warp 32 x 32 tile, padded against bank conflicts
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
@@ -194,46 +202,66 @@ __global__ void __launch_bounds__(kThreads, 1)
     const bool have = mbar_wait(done, 0, g.err, 2u) && nk > 0;
     tc_fence_after();
 
-    const int m = m0 + warp * 32 + lane;
+    const int quad = warp & 3, half = warp >> 2;
+    const int m = m0 + quad * 32 + lane;
+    const bool mrow = m < g.M;
     float loss = 0.f;
+    float(*st)[33] = stage[warp];
     if (have) {
 #pragma unroll 1
-        for (int cc = 0; cc < kBN / 16; cc++) {
-            float v[16];
-            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cc * 16), v);
-            if (m >= g.M) continue;
+        for (int cc = half * (kBN / 64); cc < (half + 1) * (kBN / 64); cc++) {
+            float v[32];
+            tmem_ld32(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(cc * 32), v);
+            const int nb = n0 + cc * 32;
+            // lane = row m: outputs indexed [n][m] are coalesced across lanes
 #pragma unroll
-            for (int j = 0; j < 16; j++) {
-                const int n = n0 + cc * 16 + j;
-                if (n >= g.N) continue;
-                const size_t mn = (size_t)m * g.N + n, nm = (size_t)n * g.M + m;
+            for (int j = 0; j < 32; j++) {
+                const int n = nb + j;
+                const bool ok = mrow && n < g.N;
+                const size_t nm = (size_t)n * g.M + m;
+                float r = 0.f;  // value of the row-major BF16 output
                 if (EPI == kEpiF32) {
-                    g.out_f32[(size_t)blockIdx.z * g.M * g.N + mn] = v[j];
+                    if (ok) g.out_f32[(size_t)blockIdx.z * g.M * g.N + nm] = v[j];
                 } else if (EPI == kEpiFwdGelu) {
-                    const float z = v[j] + g.bias[n];
-                    g.out_f32[mn] = z;
-                    const __nv_bfloat16 h = __float2bfloat16_rn(gelu(z));
-                    g.out_bf[mn] = h;
-                    g.out_bfT[nm] = h;
+                    if (ok) {
+                        const float z = v[j] + g.bias[n];
+                        g.out_f32[nm] = z;
+                        r = gelu(z);
+                        g.out_bfT[nm] = __float2bfloat16_rn(r);
+                    }
                 } else if (EPI == kEpiFwdOut) {
-                    const float y = v[j] + g.bias[n];
-                    g.out_f32[mn] = y;
-                    if (g.target) {
-                        float d = 0.f;
-                        if (n < g.n_valid && m < g.m_valid) {
-                            const float e = y - g.target[mn];
-                            loss += g.tweight[n] * e * e;
-                            d = g.grad_scale * g.tweight[n] * e;
+                    if (ok) {
+                        const float y = v[j] + g.bias[n];
+                        g.out_f32[nm] = y;
+                        if (g.target) {
+                            if (n < g.n_valid && m < g.m_valid) {
+                                const float e = y - g.target[nm];
+                                loss += g.tweight[n] * e * e;
+                                r = g.grad_scale * g.tweight[n] * e;
+                            }
+                            g.out_bfT[nm] = __float2bfloat16_rn(r);
                         }
-                        const __nv_bfloat16 db = __float2bfloat16_rn(d);
-                        g.out_bf[mn] = db;
-                        g.out_bfT[nm] = db;
                     }
                 } else {  // kEpiBwdGelu
-                    const __nv_bfloat16 dz = __float2bfloat16_rn(v[j] * gelu_grad(g.zin[mn]));
-                    g.out_bf[mn] = dz;
-                    g.out_bfT[nm] = dz;
+                    if (ok) {
+                        r = v[j] * gelu_grad(g.zin[nm]);
+                        g.out_bfT[nm] = __float2bfloat16_rn(r);
+                    }
                 }
+                st[lane][j] = r;
+            }
+            // row-major BF16 output [m][n]: through the padded tile, one row per
+            // instruction (lane = column)
+            const bool rowmajor = EPI == kEpiFwdGelu || EPI == kEpiBwdGelu || (EPI == kEpiFwdOut && g.target);
+            if (rowmajor) {
+                __syncwarp();
+                const int n = nb + lane;
+#pragma unroll 4
+                for (int rr = 0; rr < 32; rr++) {
+                    const int mr = m0 + quad * 32 + rr;
+                    if (mr < g.M && n < g.N) g.out_bf[(size_t)mr * g.N + n] = __float2bfloat16_rn(st[rr][lane]);
+                }
+                __syncwarp();
             }
         }
     } else if (threadIdx.x == 0) {
@@ -248,7 +276,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     tc_fence_before();
     __syncthreads();
     if (EPI == kEpiFwdOut && g.target && g.loss_part && threadIdx.x == 0)
-        g.loss_part[blockIdx.x * gridDim.y + blockIdx.y] = red[0] + red[1] + red[2] + red[3];
+        g.loss_part[blockIdx.x * gridDim.y + blockIdx.y] =
+            ((red[0] + red[1]) + (red[2] + red[3])) + ((red[4] + red[5]) + (red[6] + red[7]));
     if (warp == 0) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kBN));

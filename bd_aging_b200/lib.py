@@ -16,7 +16,7 @@ from dataclasses import dataclass
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libbd_aging_b200.so")
+LIB_PATH = os.environ.get("BD_AGING_LIB") or os.path.join(HERE, "libbd_aging_b200.so")
 
 BD_OK, BD_ERR_ARG, BD_ERR_CUDA, BD_ERR_CELL_OVERFLOW, BD_ERR_NOMEM, BD_ERR_STATE = 0, 1, 2, 3, 4, 5
 BD_ERR_TIMEOUT, BD_ERR_FILE, BD_ERR_FORMAT, BD_ERR_NUMERIC = 6, 7, 8, 9
@@ -57,7 +57,8 @@ class SystemDesc(C.Structure):
 class EngineOpts(C.Structure):
     _fields_ = [("rng", C.c_int), ("cell_capacity", C.c_int), ("brick", C.c_int * 3), ("threads", C.c_int),
                 ("mode", C.c_int), ("cluster", C.c_int), ("autotune", C.c_int), ("graph_steps", C.c_int),
-                ("qmax", C.c_float), ("ni_start", C.c_longlong), ("rng_stream", C.c_uint)]
+                ("qmax", C.c_float), ("ni_start", C.c_longlong), ("rng_stream", C.c_uint),
+                ("neighbor_skin", C.c_float)]
 
 
 class Observables(C.Structure):
@@ -82,7 +83,8 @@ class EngineInfo(C.Structure):
     _fields_ = [("nsys", C.c_int), ("n_particles", C.c_longlong), ("n_cells", C.c_longlong),
                 ("brick", C.c_int * 3), ("threads", C.c_int), ("cell_capacity", C.c_int),
                 ("staging_capacity", C.c_int), ("mode", C.c_int), ("cluster", C.c_int),
-                ("smem_bytes", C.c_size_t), ("next_step", C.c_longlong)]
+                ("smem_bytes", C.c_size_t), ("next_step", C.c_longlong), ("neighbor_skin", C.c_float),
+                ("list_builds", C.c_longlong)]
 
 
 _LIB = None
@@ -352,8 +354,9 @@ class System:
 class Engine:
     """Batched replica engine (bd_engine_*)."""
 
-    def __init__(self, systems, rng="philox", mode="auto", brick=None, threads=0, cell_capacity=16,
-                 graph_steps=96, qmax=2 * np.pi, ni_start=0, rng_stream=0, cluster=0, autotune=0):
+    def __init__(self, systems, rng="philox", mode="auto", brick=None, threads=0, cell_capacity=0,
+                 graph_steps=96, qmax=2 * np.pi, ni_start=0, rng_stream=0, cluster=0, autotune=0,
+                 neighbor_skin=None):
         self.systems = list(systems)
         n = len(self.systems)
         arr = (SystemDesc * n)(*[s.desc() for s in self.systems])
@@ -371,6 +374,8 @@ class Engine:
         o.rng_stream = rng_stream
         o.cluster = cluster
         o.autotune = autotune
+        if neighbor_skin is not None:  # None: the library default
+            o.neighbor_skin = neighbor_skin
         h = _vp()
         _check(_lib().bd_engine_create(arr, n, C.byref(o), C.byref(h)), "bd_engine_create")
         self._h = h

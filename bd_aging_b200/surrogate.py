@@ -193,21 +193,37 @@ def fs_at(settings, tw, lag, k, seeds, n_per_replica=1000, dt=1e-4):
     return fs, X, Y
 
 
-def crossing_study(phi=0.52, tw=100, lag=400, k=7.0, budget=6, seeds=(1, 2, 3, 4), t_range=(0.05, 1.0),
-                   truth_points=24, pretrain=None, fit_steps=1500, n_per_replica=1000, dt=1e-4):
-    """Locate T* with F_s(k; t_w, t_w + lag) = 0.5 with `budget` simulated
-    temperatures, by a uniform grid and by surrogate proposals (half the
-    budget on a coarse grid, the rest proposed one at a time, each simulated
-    and added to the training set).  The truth is a dense plain sweep.
-    Returns a dict of estimates and errors."""
+def line_crossing(ts, fs, target, center, half_width):
+    """Least-squares line through the points within center +- half_width
+    (at least the three nearest), solved for fs = target."""
+    ts, fs = np.asarray(ts, np.float64), np.asarray(fs, np.float64)
+    d = np.abs(ts - center)
+    sel = d <= half_width
+    if sel.sum() < 3:
+        sel = np.zeros(len(ts), bool)
+        sel[np.argsort(d)[:3]] = True
+    b, a = np.polyfit(ts[sel], fs[sel], 1)
+    return float((target - a) / b) if b != 0 else float(center)
+
+
+def crossing_study(phi=0.52, tw=100, lag=3000, k=7.0, budget=6, seeds=(1, 2, 3, 4), t_range=(0.05, 1.0),
+                   truth_points=24, pretrain=None, fit_steps=1500, n_per_replica=1000, dt=1e-4, target=0.5):
+    """Locate T* with F_s(k; t_w, t_w + lag) = target with `budget` simulated
+    temperatures, (a) by a uniform grid and linear interpolation between the
+    bracketing grid points, (b) with the surrogate: half the budget on a
+    coarse grid, then proposals at the network's crossing and around it
+    (each simulated, added to the training set, the network refitted), the
+    estimate a least-squares line through the simulated points near the
+    proposals.  The truth is a dense plain sweep.  The simulations judge:
+    both estimates use simulated values only."""
     log_tw, log_t = math.log10(max(tw, 1) * dt), math.log10(lag * dt)
     ts_truth = np.linspace(t_range[0], t_range[1], truth_points)
     f_truth, _, _ = fs_at([(phi, t) for t in ts_truth], tw, lag, k, seeds, n_per_replica, dt)
-    t_star = crossing(ts_truth, f_truth, 0.5)
+    t_star = crossing(ts_truth, f_truth, target)
     # uniform grid
     ts_grid = np.linspace(t_range[0], t_range[1], budget)
     f_grid, _, _ = fs_at([(phi, t) for t in ts_grid], tw, lag, k, seeds, n_per_replica, dt)
-    t_grid = crossing(ts_grid, f_grid, 0.5)
+    t_grid = crossing(ts_grid, f_grid, target)
     # surrogate: coarse grid, then proposals
     n0 = max(2, budget // 2)
     ts_s = list(np.linspace(t_range[0], t_range[1], n0))
@@ -217,12 +233,13 @@ def crossing_study(phi=0.52, tw=100, lag=400, k=7.0, budget=6, seeds=(1, 2, 3, 4
         X, Y = np.concatenate([pretrain[0], X]), np.concatenate([pretrain[1], Y])
     model = SurrogateModel(seed=5)
     model.fit(X, Y, steps=fit_steps)
-    proposals = []
-    for _ in range(budget - n0):
-        tp = propose_temperature(model, phi, log_tw, log_t, k, 0.5, t_range)
-        tp = float(np.clip(tp, t_range[0], t_range[1]))
-        if min(abs(tp - t) for t in ts_s) < 1e-3:  # already simulated: step to the bracket's midpoint
-            tp = 0.5 * (tp + sorted(ts_s, key=lambda t: abs(t - tp))[1])
+    spacing = (t_range[1] - t_range[0]) / (n0 - 1)
+    offsets = [0.0, -0.25, 0.25, -0.5, 0.5]  # in units of the coarse spacing / 2
+    proposals, center = [], None
+    for i in range(budget - n0):
+        c = propose_temperature(model, phi, log_tw, log_t, k, target, t_range)
+        center = c if center is None else c
+        tp = float(np.clip(c + offsets[i % len(offsets)] * spacing * 0.5, t_range[0], t_range[1]))
         proposals.append(tp)
         fp, Xp, Yp = fs_at([(phi, tp)], tw, lag, k, seeds, n_per_replica, dt)
         ts_s.append(tp)
@@ -230,6 +247,7 @@ def crossing_study(phi=0.52, tw=100, lag=400, k=7.0, budget=6, seeds=(1, 2, 3, 4
         X, Y = np.concatenate([X, Xp]), np.concatenate([Y, Yp])
         model.fit(X, Y, steps=fit_steps // 2)
     model.close()
-    t_sur = crossing(ts_s, f_s, 0.5)  # the simulations judge: interpolate simulated values
+    t_sur = line_crossing(ts_s, f_s, target, center, 0.3 * spacing)
     return {"t_star": t_star, "grid": t_grid, "surrogate": t_sur, "err_grid": abs(t_grid - t_star),
-            "err_surrogate": abs(t_sur - t_star), "proposals": proposals, "budget": budget}
+            "err_surrogate": abs(t_sur - t_star), "proposals": proposals, "budget": budget,
+            "f_truth": [float(v) for v in f_truth], "ts_truth": [float(v) for v in ts_truth]}

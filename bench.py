@@ -56,6 +56,8 @@ def parse():
                     help="one launch per time step, or persistent cluster launches of many steps")
     ap.add_argument("--cluster", type=int, default=0, help="CTAs per cluster in persistent mode")
     ap.add_argument("--autotune", action="store_true", help="time brick shapes during warm-up, keep the fastest")
+    ap.add_argument("--skin", type=float, default=None,
+                    help="neighbour-list skin (0: sweep every step; default: the library's)")
     return ap.parse_args()
 
 
@@ -64,6 +66,7 @@ def workload_systems(name, replicas, rank):
     """Returns (systems, description dict). Seeds differ per rank."""
     from bd_aging_b200 import configs as CF
     from bd_aging_b200 import lib as B
+    from bd_aging_b200 import ranks
     sb, ss = float(CF.SIGMA_BIG), float(CF.SIGMA_SML)
     rng = np.random.default_rng(1000 + rank)
     out = []
@@ -72,7 +75,7 @@ def workload_systems(name, replicas, rank):
         side = float(np.float32(CF.side_from_phi(nb, ns, 0.58)))
         for r in range(replicas):
             out.append(B.System(n_big=nb, n_sml=ns, side=side, sigma_big=sb, sigma_sml=ss, dt=1e-5, T0=1.0, Tf=0.1,
-                                t0=0.0, tf=1e-30, protocol="linear", seed=1 + r + 100000 * rank))
+                                t0=0.0, tf=1e-30, protocol="linear", seed=ranks.replica_seed(1, r, rank)))
         desc = {"workload": "aging quench N=32768 phi=0.58 T 1.0->0.1 dt=1e-5, %d replicas batched" % replicas,
                 "n_per_replica": 32768, "replicas": replicas, "phi": 0.58}
     elif name == "batched":
@@ -82,20 +85,20 @@ def workload_systems(name, replicas, rank):
             tfin = float(rng.uniform(0.05, 1.0))
             side = float(np.float32(CF.side_from_phi(n // 2, n // 2, phi)))
             out.append(B.System(n_big=n // 2, n_sml=n // 2, side=side, sigma_big=sb, sigma_sml=ss, dt=1e-5, T0=1.0,
-                                Tf=tfin, t0=0.0, tf=1e-30, protocol="linear", seed=7 + r + 100000 * rank))
+                                Tf=tfin, t0=0.0, tf=1e-30, protocol="linear", seed=ranks.replica_seed(7, r, rank)))
         desc = {"workload": "256 ragged replicas N in [500,8000] phi in [0.50,0.60] T_final in [0.05,1.0] dt=1e-5",
                 "replicas": 256}
     elif name == "large":
         nb = ns = 524288
         side = float(np.float32(CF.side_from_phi(nb, ns, 0.58)))
         out.append(B.System(n_big=nb, n_sml=ns, side=side, sigma_big=sb, sigma_sml=ss, dt=1e-5, T0=0.2,
-                            protocol="const", seed=3 + 100000 * rank))
+                            protocol="const", seed=ranks.replica_seed(3, 0, rank)))
         desc = {"workload": "large single system N=1048576 phi=0.58 T=0.2 dt=1e-5", "replicas": 1}
     else:
         nb = ns = 500
         side = float(np.float32(CF.side_from_phi(nb, ns, 0.50)))
         out.append(B.System(n_big=nb, n_sml=ns, side=side, sigma_big=sb, sigma_sml=ss, dt=2e-5, T0=1.0,
-                            protocol="const", seed=1 + 100000 * rank))
+                            protocol="const", seed=ranks.replica_seed(1, 0, rank)))
         desc = {"workload": "small N=1000 phi=0.50 T=1.0 dt=2e-5 single replica", "replicas": 1}
     return out, desc
 
@@ -175,10 +178,11 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
-def profile_traffic_per_particle_step():
+def profile_traffic_per_particle_step(list_mode=False):
     """DRAM bytes per particle-step of the step kernel from the committed ncu
-    summary (profiles/k_step_aging.md, line 'dram_bytes_per_particle_step: X')."""
-    p = os.path.join(ROOT, "profiles", "k_step_aging.md")
+    summary (profiles/k_step_list_aging.md in neighbour-list mode, else
+    profiles/k_step_aging.md; line 'dram_bytes_per_particle_step: X')."""
+    p = os.path.join(ROOT, "profiles", "k_step_list_aging.md" if list_mode else "k_step_aging.md")
     if not os.path.exists(p):
         return None
     for ln in open(p):
@@ -275,6 +279,43 @@ def correlator_leg(eng, P, slots=16, iters=20, q=6.19):
             "bytes_per_call": traffic, "note": "call time includes the host read-back of the sums"}
 
 
+def precision_leg(n=8192, phi=0.58, steps=1000, temp=0.1, dt=1e-5, seed=5, q=7.0):
+    """Observables after 10^3 steps of one replica (config-2 conditions after
+    the quench: phi=0.58, T=0.1, dt=1e-5; N=8192 so the host FP64 run stays
+    within seconds) from the engine and from host runs in FP64 and at the
+    reference's FP32 precision, all with the engine's Philox noise and the
+    same relaxed start.  Errors are relative to the FP64 run."""
+    from bd_aging_b200 import configs as CF
+    from bd_aging_b200 import lib as B
+    from oracle import oracle as O
+    sb, ss = float(CF.SIGMA_BIG), float(CF.SIGMA_SML)
+    nb = ns = n // 2
+    side = float(np.float32(CF.side_from_phi(nb, ns, phi)))
+    relax = B.System(n_big=nb, n_sml=ns, side=side, sigma_big=sb, sigma_sml=ss, dt=1e-4, seed=99, T0=1.0,
+                     protocol="const", force_cap=100.0)
+    e = B.Engine([relax], rng_stream=1)
+    e.set_positions(CF.uniform_config(nb, ns, side, seed))
+    e.run(1500)
+    pos, _ = e.get_positions()
+    e.close()
+    sysd = B.System(n_big=nb, n_sml=ns, side=side, sigma_big=sb, sigma_sml=ss, dt=dt, seed=seed, T0=temp,
+                    protocol="const")
+    e = B.Engine([sysd], qmax=q)
+    e.set_positions(pos)
+    e.run(steps)
+    o = e.observe()[0]
+    e.close()
+    keys = ("msd_big", "msd_sml", "fself_big", "energy_big", "energy_sml", "virial")
+    mb, ms = float(np.float32(1) / np.float32(sb)), float(np.float32(1) / np.float32(ss))
+    args = (pos, nb, side, sb, ss, mb, ms, dt, temp, seed, steps, q)
+    f64, _ = O.precision_run("fp64", *args)
+    f32, _ = O.precision_run("fp32_reference", *args)
+    return {"workload": "N=%d phi=%.2f T=%.2f dt=%g, %d steps, Philox noise" % (n, phi, temp, dt, steps),
+            "fp64": {k: float(f64[k]) for k in keys},
+            "engine_rel_err": {k: abs(o[k] - f64[k]) / abs(f64[k]) for k in keys},
+            "fp32_reference_rel_err": {k: abs(f32[k] - f64[k]) / abs(f64[k]) for k in keys}}
+
+
 SURROGATE_SIZES = [(256, 5)] + [(256, 256)] * 3 + [(34, 256)]       # live (N, K) per layer
 SURROGATE_PADDED = [(256, 64)] + [(256, 256)] * 3 + [(128, 256)]    # as executed (K and N padded)
 
@@ -353,35 +394,26 @@ def run_ours(args):
         return run_surrogate_only(args)
     import torch
     from bd_aging_b200 import lib as B
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
+    from bd_aging_b200 import ranks
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    rank, world, local = ranks.init("nccl")
     systems, desc = workload_systems(args.workload, args.replicas, rank)
     pos = relaxed_positions(systems, 777 + rank, args.relax_steps)
     P = sum(s.n for s in systems)
     S = args.md_steps
     eng = B.Engine(systems, graph_steps=96, brick=args.brick, threads=args.threads, mode=args.mode,
-                   cluster=args.cluster, autotune=int(args.autotune))
+                   cluster=args.cluster, autotune=int(args.autotune), neighbor_skin=args.skin)
     eng.set_positions(pos)
     for _ in range(args.warmup):
         eng.run(S)
     info = eng.info()  # after warm-up: the autotuner may have changed the layout
     clocks = ClockSampler(local)
     clocks.start()
-    if dist:
-        dist.barrier()
+    ranks.barrier()
     ms = cuda_time(eng, lambda: eng.run(S), args.steps)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
+    ms = ranks.max_over_ranks(ms)
+    ranks.barrier()
     ck = clocks.stop()
     total_ps = P * S * args.steps * world
     value = total_ps / (ms / 1e3)
@@ -389,7 +421,11 @@ def run_ours(args):
     avg_launch_s = (ms / 1e3) / launches
     peak, peak_kind = measured_peak_hbm()
     achieved = ALG_BYTES_PER_PARTICLE_STEP * P / avg_launch_s / 1e9
-    tpp = profile_traffic_per_particle_step()
+    list_mode = info.neighbor_skin > 0
+    tpp = profile_traffic_per_particle_step(list_mode)
+    # kernels per time step: the list step plus its four rebuild kernels (which
+    # exit at once when no list is stale), or the one sweep kernel
+    per_step = 5 if list_mode else (1 if args.mode == "plain" else 0)
     line = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 forces, f32+compensation positions, f64 displacement",
@@ -398,8 +434,9 @@ def run_ours(args):
                            l2="inputs larger than L2" if P * 112 > 126e6 else "state fits in L2",
                            brick=list(info.brick), threads=info.threads, cell_capacity=info.cell_capacity,
                            mode=args.mode, cluster=info.cluster if args.mode == "persistent" else None,
+                           neighbor_skin=info.neighbor_skin, list_builds=info.list_builds,
                            autotune=bool(args.autotune)),
-            "gpu_launches": int(args.steps * (math.ceil(S / 96) + (S if args.mode == "plain" else math.ceil(S / 96)))),
+            "gpu_launches": int(args.steps * (math.ceil(S / 96) * (1 if per_step else 2) + per_step * S)),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "alg_bytes_per_launch": ALG_BYTES_PER_PARTICLE_STEP * P,
@@ -408,7 +445,7 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_extras:
         # plain single-replica engine, same system
         s1 = systems[0]
-        e1 = B.Engine([s1], graph_steps=96, brick=args.brick, threads=args.threads)
+        e1 = B.Engine([s1], graph_steps=96, brick=args.brick, threads=args.threads, neighbor_skin=args.skin)
         e1.set_positions(pos[: s1.n])
         e1.run(S)
         k1 = max(3, args.steps)
@@ -438,10 +475,10 @@ def run_ours(args):
         line["cpu_baseline"] = cpu_baseline()
         line["correlator"] = correlator_leg(eng, P)
         eng.close()
+        line["precision"] = precision_leg()
         line["surrogate"] = surrogate_leg()
     eng.close()
-    if dist:
-        dist.destroy_process_group()
+    ranks.finalize()
     if rank == 0:
         print(json.dumps(line))
 

@@ -237,7 +237,7 @@ typedef struct bd_system_desc {
 
 typedef struct bd_engine_opts {
     int rng;                   /* BD_RNG_* */
-    int cell_capacity;         /* slots per cell (0 = 16, at most 16) */
+    int cell_capacity;         /* slots per cell (0 = 16, 24 in list mode; at most 24) */
     int brick[3];              /* cells per brick (0 = autotune / default) */
     int threads;               /* CTA size (0 = default) */
     int mode;                  /* BD_MODE_* */
@@ -248,6 +248,10 @@ typedef struct bd_engine_opts {
     long long ni_start;        /* reference step index of the first update
                                   (-ntrans, main.cu:407 and 494) */
     unsigned rng_stream;       /* Philox stream number (0 dynamics, 1 relaxation) */
+    float neighbor_skin;       /* > 0 (default 0.25): neighbour-list mode (plain mode,
+                                  generated noise): lists of partners within cut + skin,
+                                  rebuilt on the device when a particle of the replica
+                                  has moved skin / 2; 0: the 27-cell sweep every step */
 } bd_engine_opts;
 
 typedef struct bd_observables {
@@ -265,6 +269,8 @@ typedef struct bd_engine_info {
     int brick[3], threads, cell_capacity, staging_capacity, mode, cluster;
     size_t smem_bytes;
     long long next_step;          /* reference ni of the next update */
+    float neighbor_skin;          /* 0 when the engine sweeps every step */
+    long long list_builds;        /* neighbour-list builds so far */
 } bd_engine_info;
 
 void bd_engine_opts_default(bd_engine_opts *opts);

@@ -534,3 +534,182 @@ void or_eng_fself_msd(int n, const double *d, double q, double *fs, double *msd)
     *fs = sf / n;
     *msd = sm / n;
 }
+
+/* ------------------------------------------------------------------------
+ * Precision study (FP32 + compensated positions and FP64 displacements vs
+ * an FP64 run and a run at the reference's FP32 precision).  All three use
+ * the engine's Philox noise (or_eng_gauss3 of seed, particle index, step,
+ * stream), the same WCA pair (potentials.cu:137-147 with per-species-pair
+ * cut distances) and the update d = F mob dt + amp xi (update_ermak.cu:
+ * 122-141); they differ only in arithmetic.  Forces use a cell list (cell
+ * side >= the largest cut distance) or all pairs when the box holds fewer
+ * than 3 cells.  obs: msd_big, msd_sml, fself_big(q), energy_big,
+ * energy_sml (0.5 sum pot / N), virial (sum vir_i).  dsp_out: [3n]
+ * unwrapped displacement. */
+typedef struct { int nc; int *head, *next, *cell; } or_cells;
+
+static void cells_build_d(or_cells *c, int n, const double *pos, double side, double rcmax) {
+    c->nc = (int)floor(side / rcmax);
+    if (c->nc < 3) { c->nc = 0; return; }
+    int nc3 = c->nc * c->nc * c->nc;
+    for (int i = 0; i < nc3; i++) c->head[i] = -1;
+    for (int m = 0; m < n; m++) {
+        int ix[3];
+        for (int k = 0; k < 3; k++) {
+            ix[k] = (int)(pos[3 * m + k] / side * c->nc);
+            if (ix[k] < 0) ix[k] = 0;
+            if (ix[k] >= c->nc) ix[k] = c->nc - 1;
+        }
+        int ci = ix[0] + c->nc * (ix[1] + c->nc * ix[2]);
+        c->cell[m] = ci;
+        c->next[m] = c->head[ci];
+        c->head[ci] = m;
+    }
+}
+
+static void pair_d(double s, double dx, double dy, double dz, double *f, double *pot, double *vir) {
+    double d2 = dx * dx + dy * dy + dz * dz;
+    if (!(d2 < s * s)) return;
+    double di = 1.0 / sqrt(d2), sor = s * di, s6 = sor * sor * sor;
+    s6 *= s6;
+    double s12 = s6 * s6, nf = -12.0 * (s12 - s6) * di;
+    *pot += s12 - 2.0 * s6 + 1.0;
+    double px = nf * di * dx, py = nf * di * dy, pz = nf * di * dz;
+    f[0] += px; f[1] += py; f[2] += pz;
+    *vir -= 0.5 * (dx * px + dy * py + dz * pz);
+}
+
+static void forces_d(int n, int n_big, const double *pos, double side, const double sig[3], or_cells *c, double *ff,
+                     double *pot, double *vir) {
+    double rcmax = sig[0] > sig[2] ? sig[0] : sig[2];
+    if (sig[1] > rcmax) rcmax = sig[1];
+    cells_build_d(c, n, pos, side, rcmax * (1.0 + 1e-9));
+    const double half = 0.5 * side;  /* positions lie in [0, side): one image shift at most */
+    for (int m = 0; m < n; m++) {
+        double f[3] = {0, 0, 0}, pm = 0, vm = 0;
+        int tm = m >= n_big;
+        if (c->nc) {
+            int nc = c->nc, ci = c->cell[m];
+            int cx = ci % nc, cy = (ci / nc) % nc, cz = ci / (nc * nc);
+            for (int oz = -1; oz <= 1; oz++)
+                for (int oy = -1; oy <= 1; oy++)
+                    for (int ox = -1; ox <= 1; ox++) {
+                        int gx = (cx + ox + nc) % nc, gy = (cy + oy + nc) % nc, gz = (cz + oz + nc) % nc;
+                        for (int j = c->head[gx + nc * (gy + nc * gz)]; j >= 0; j = c->next[j]) {
+                            if (j == m) continue;
+                            double d[3];
+                            for (int k = 0; k < 3; k++) {
+                                d[k] = pos[3 * j + k] - pos[3 * m + k];
+                                if (d[k] > half) d[k] -= side;
+                                else if (d[k] < -half) d[k] += side;
+                            }
+                            pair_d(sig[tm + (j >= n_big)], d[0], d[1], d[2], f, &pm, &vm);
+                        }
+                    }
+        } else {
+            for (int j = 0; j < n; j++) {
+                if (j == m) continue;
+                double d[3];
+                for (int k = 0; k < 3; k++) {
+                    d[k] = pos[3 * j + k] - pos[3 * m + k];
+                    d[k] -= side * floor(d[k] / side + 0.5);
+                }
+                pair_d(sig[tm + (j >= n_big)], d[0], d[1], d[2], f, &pm, &vm);
+            }
+        }
+        ff[3 * m] = f[0]; ff[3 * m + 1] = f[1]; ff[3 * m + 2] = f[2];
+        pot[m] = pm;
+        vir[m] = vm;
+    }
+}
+
+static void observables_d(int n, int n_big, const double *dsp, const double *pot, const double *vir, double q,
+                          double *obs) {
+    double msd[2] = {0, 0}, fs = 0, e[2] = {0, 0}, w = 0;
+    for (int m = 0; m < n; m++) {
+        int t = m >= n_big;
+        double r2 = dsp[3 * m] * dsp[3 * m] + dsp[3 * m + 1] * dsp[3 * m + 1] + dsp[3 * m + 2] * dsp[3 * m + 2];
+        msd[t] += r2;
+        if (!t) {
+            double qr = q * sqrt(r2);
+            fs += qr > 0 ? sin(qr) / qr : 1.0;
+        }
+        e[t] += 0.5 * pot[m];
+        w += vir[m];
+    }
+    int ns = n - n_big;
+    obs[0] = n_big ? msd[0] / n_big : 0;
+    obs[1] = ns ? msd[1] / ns : 0;
+    obs[2] = n_big ? fs / n_big : 0;
+    obs[3] = n_big ? e[0] / n_big : 0;
+    obs[4] = ns ? e[1] / ns : 0;
+    obs[5] = w;
+}
+
+static int cells_alloc(or_cells *c, int n, double side, double rcmax) {
+    int nc = (int)floor(side / rcmax);
+    size_t nc3 = nc >= 3 ? (size_t)nc * nc * nc : 1;
+    c->head = (int *)malloc(sizeof(int) * nc3);
+    c->next = (int *)malloc(sizeof(int) * n);
+    c->cell = (int *)malloc(sizeof(int) * n);
+    return c->head && c->next && c->cell;
+}
+static void cells_free(or_cells *c) { free(c->head); free(c->next); free(c->cell); }
+
+/* mode 0: FP64 everything.  mode 1: reference precision: float positions
+ * (wrapped with side_inv = 1/side in float) and float unwrapped positions
+ * rr_raw, float displacement d = (F mob) dt + amp xi with float forces from
+ * the FP64 pair routine rounded to float, float amp (update_ermak.cu:114). */
+int or_precision_run(int mode, int n, int n_big, const float *pos0, double side, double sig_big, double sig_sml,
+                     double mob_big, double mob_sml, double dt, double temp, uint64_t seed, uint32_t stream,
+                     long long ni0, int steps, double q, double *obs, double *dsp_out) {
+    double sig[3] = {sig_big, 0.5 * (sig_big + sig_sml), sig_sml};
+    double *pos = (double *)malloc(sizeof(double) * 3 * n), *ff = (double *)malloc(sizeof(double) * 3 * n);
+    double *pot = (double *)malloc(sizeof(double) * n), *vir = (double *)malloc(sizeof(double) * n);
+    double *dsp = (double *)calloc(3 * (size_t)n, sizeof(double));
+    float *rr = (float *)malloc(sizeof(float) * 3 * n), *raw = (float *)malloc(sizeof(float) * 3 * n);
+    or_cells c;
+    double rcmax = sig_big > sig_sml ? sig_big : sig_sml;
+    if (!pos || !ff || !pot || !vir || !dsp || !rr || !raw || !cells_alloc(&c, n, side, rcmax * (1.0 + 1e-9))) return 1;
+    for (int i = 0; i < 3 * n; i++) { pos[i] = pos0[i]; rr[i] = pos0[i]; raw[i] = pos0[i]; }
+    const float fside = (float)side, fside_inv = 1.0f / fside, fdt = (float)dt;
+    for (int s = 0; s < steps; s++) {
+        if (mode == 1)
+            for (int i = 0; i < 3 * n; i++) pos[i] = rr[i];
+        forces_d(n, n_big, pos, side, sig, &c, ff, pot, vir);
+        long long ni = ni0 + s;
+        for (int m = 0; m < n; m++) {
+            int t = m >= n_big;
+            double mob = t ? mob_sml : mob_big, xi[3];
+            or_eng_gauss3(seed, (uint32_t)m, (uint64_t)ni, stream, xi);
+            if (mode == 0) {
+                double amp = sqrt(2.0 * temp * mob * dt);
+                for (int k = 0; k < 3; k++) {
+                    double d = ff[3 * m + k] * mob * dt + amp * xi[k];
+                    pos[3 * m + k] += d;
+                    pos[3 * m + k] -= side * floor(pos[3 * m + k] / side);
+                    dsp[3 * m + k] += d;
+                }
+            } else {
+                float amp = (float)sqrt(2.0 * temp * (double)(float)mob * dt), fm = (float)mob;
+                for (int k = 0; k < 3; k++) {
+                    float d = (float)ff[3 * m + k] * fm * fdt + amp * (float)xi[k];
+                    rr[3 * m + k] += d;
+                    raw[3 * m + k] += d;
+                    rr[3 * m + k] -= fside * floorf(fside_inv * rr[3 * m + k]);
+                }
+            }
+        }
+    }
+    if (mode == 1)
+        for (int i = 0; i < 3 * n; i++) {
+            pos[i] = rr[i];
+            dsp[i] = (double)(raw[i] - pos0[i]);
+        }
+    forces_d(n, n_big, pos, side, sig, &c, ff, pot, vir);
+    observables_d(n, n_big, dsp, pot, vir, q, obs);
+    if (dsp_out) memcpy(dsp_out, dsp, sizeof(double) * 3 * n);
+    cells_free(&c);
+    free(pos); free(ff); free(pot); free(vir); free(dsp); free(rr); free(raw);
+    return 0;
+}

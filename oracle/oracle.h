@@ -50,6 +50,9 @@ int or_ref_sampling_indexes(float minimal_decade, float run_time, float dt, int 
 typedef struct { uint64_t useed[250]; uint64_t uuy; int np, nq, init; } or_rannew64_state;
 void or_rannew64_seed(or_rannew64_state *s, long idum);
 void or_rannew64_particle_noise(long long seed, int n, int steps, float *noise);
+int or_precision_run(int mode, int n, int n_big, const float *pos0, double side, double sig_big, double sig_sml,
+                     double mob_big, double mob_sml, double dt, double temp, uint64_t seed, uint32_t stream,
+                     long long ni0, int steps, double q, double *obs, double *dsp_out);
 double or_rannew64_next(or_rannew64_state *s);
 /* Contracting_Vector3D::add_statistics (Contracting_Vector3D.cu:57-164) in the
  * reference's float arithmetic; ata: 3 x bins x bins, atb: 3 x bins. side<=0:

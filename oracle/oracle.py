@@ -81,6 +81,10 @@ def oracle_lib():
         L.or_ref_sampling_indexes.restype = C.c_int
         L.or_rannew64_next.restype = C.c_double
         L.or_rannew64_particle_noise.argtypes = [C.c_longlong, C.c_int, C.c_int, _f32p]
+        L.or_precision_run.argtypes = [C.c_int, C.c_int, C.c_int, _f32p, C.c_double, C.c_double, C.c_double,
+                                       C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64, C.c_uint32,
+                                       C.c_longlong, C.c_int, C.c_double, _f64p, _f64p]
+        L.or_precision_run.restype = C.c_int
         L.or_ref_cv3d_add.argtypes = [C.c_int, C.c_float, _f32p, _f32p, C.c_int, C.c_float, _f32p, _f32p]
         L.or_ref_cv3d_add.restype = C.c_int
         L.or_philox4x32_10.argtypes = [_u32p, _u32p, _u32p]
@@ -101,6 +105,24 @@ def rannew64_particle_noise(seed: int, n: int, steps: int) -> np.ndarray:
     out = np.zeros((steps, n, 3), np.float32)
     oracle_lib().or_rannew64_particle_noise(int(seed), int(n), int(steps), out)
     return out
+
+
+PRECISION_FIELDS = ("msd_big", "msd_sml", "fself_big", "energy_big", "energy_sml", "virial")
+
+
+def precision_run(mode, pos, n_big, side, sig_big, sig_sml, mob_big, mob_sml, dt, temp, seed, steps, q,
+                  stream=0, ni0=0):
+    """mode "fp64" or "fp32_reference": observables after `steps` steps with
+    the engine's Philox noise, and the FP64 displacement [n, 3]."""
+    pos = np.ascontiguousarray(pos, np.float32)
+    n = len(pos)
+    obs = np.zeros(6, np.float64)
+    dsp = np.zeros((n, 3), np.float64)
+    rc = oracle_lib().or_precision_run({"fp64": 0, "fp32_reference": 1}[mode], n, n_big, pos, side, sig_big,
+                                       sig_sml, mob_big, mob_sml, dt, temp, seed, stream, ni0, steps, q, obs, dsp)
+    if rc:
+        raise MemoryError("or_precision_run")
+    return dict(zip(PRECISION_FIELDS, obs)), dsp
 
 
 def ref_available() -> bool:

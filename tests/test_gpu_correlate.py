@@ -100,7 +100,7 @@ def test_origin_slot_equals_builtin_observables():
 def test_correlations_independent_of_batching_and_mode():
     systems, pos = ragged(3, 17)
     res = []
-    for kw in (dict(), dict(mode="persistent", cluster=2)):
+    for kw in (dict(neighbor_skin=0.0), dict(mode="persistent", cluster=2)):
         e = B.Engine(systems, **kw)
         e.set_positions(pos)
         e.reserve_snapshots(2)
@@ -112,7 +112,7 @@ def test_correlations_independent_of_batching_and_mode():
     np.testing.assert_array_equal(res[0], res[1])
     off = np.cumsum([0] + [s.n for s in systems])
     for r, s in enumerate(systems):  # a replica alone gives the same bits
-        e = B.Engine([s])
+        e = B.Engine([s], neighbor_skin=0.0)
         e.set_positions(pos[off[r]:off[r + 1]])
         e.reserve_snapshots(2)
         e.snapshot(0)

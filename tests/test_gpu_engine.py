@@ -171,7 +171,7 @@ def test_persistent_cluster_mode_bit_identical_to_plain():
     ep.set_positions(pos)
     ep.run(96 + 40)  # one persistent graph chunk + one direct persistent launch
     ep.run(77)
-    e1 = B.Engine(list(systems))
+    e1 = B.Engine(list(systems), neighbor_skin=0.0)  # persistent mode sweeps every step
     e1.set_positions(pos)
     e1.run(213)
     np.testing.assert_array_equal(ep.get_positions()[0], e1.get_positions()[0])
@@ -185,7 +185,7 @@ def test_autotuner_changes_speed_not_results():
         ea = B.Engine(list(systems), mode=mode, autotune=1)
         ea.set_positions(pos)
         ea.run(300)
-        e1 = B.Engine(list(systems))
+        e1 = B.Engine(list(systems), neighbor_skin=ea.info().neighbor_skin)
         e1.set_positions(pos)
         e1.run(300)
         np.testing.assert_array_equal(ea.get_positions()[0], e1.get_positions()[0])

@@ -1,0 +1,113 @@
+"""GPU parity of the neighbour-list mode (csrc/nlist.cuh): the interacting
+pairs of every particle equal the oracle's all-pairs neighbour sets, also
+after many device-triggered rebuilds; one step matches the oracle update
+with the engine's Philox noise; list runs are deterministic (batched ==
+plain, graph == single steps); observation passes read the current state."""
+import numpy as np
+import pytest
+
+from bd_aging_b200 import configs as CF
+from bd_aging_b200 import lib as B
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+SB, SS = float(CF.SIGMA_BIG), float(CF.SIGMA_SML)
+SKIN = 0.3
+
+
+def system(nb, ns, phi, seed, **kw):
+    side = float(np.float32(CF.side_from_phi(nb, ns, phi)))
+    pos = CF.lattice_config(nb, ns, side, seed)
+    s = B.System(n_big=nb, n_sml=ns, side=side, sigma_big=SB, sigma_sml=SS, dt=kw.pop("dt", 1e-4), seed=seed,
+                 force_cap=kw.pop("force_cap", 100.0), **kw)
+    return s, pos
+
+
+def types_of(s):
+    return np.array([0] * s.n_big + [1] * s.n_sml, np.int32)
+
+
+@pytest.mark.parametrize("nb,ns,phi,brick", [(150, 150, 0.45, None), (2000, 2000, 0.55, None),
+                                             (2000, 2000, 0.55, (8, 4, 2)), (700, 300, 0.5, (3, 5, 2))])
+def test_list_neighbour_sets_bit_exact(nb, ns, phi, brick):
+    s, pos = system(nb, ns, phi, 21)
+    e = B.Engine([s], brick=brick, neighbor_skin=SKIN)
+    assert e.info().neighbor_skin == pytest.approx(SKIN)
+    e.set_positions(pos)
+    cnt, hsh = e.census()
+    _, _, _, nbr, h = O.eng_forces(pos, types_of(s), s.side, SB, SS)
+    np.testing.assert_array_equal(cnt, nbr)
+    np.testing.assert_array_equal(hsh, h)
+
+
+def test_list_sets_stay_exact_across_rebuilds():
+    s, pos = system(1500, 1500, 0.5, 31, T0=1.0)
+    e = B.Engine([s], neighbor_skin=SKIN)
+    e.set_positions(pos)
+    for k in range(3):
+        e.run(400)
+        hi, _ = e.get_positions()
+        cnt, hsh = e.census()
+        _, _, _, nbr, h = O.eng_forces(hi, types_of(s), s.side, SB, SS)
+        np.testing.assert_array_equal(cnt, nbr)
+        np.testing.assert_array_equal(hsh, h)
+    assert e.info().list_builds >= 4  # the first build plus device-triggered ones
+
+
+def test_list_one_step_matches_oracle():
+    s, pos = system(1500, 1500, 0.52, 4, T0=0.7, protocol="const", force_cap=0.0, dt=1e-5)
+    e = B.Engine([s], neighbor_skin=SKIN)
+    e.set_positions(pos)
+    e.run(1)
+    hi, raw = e.get_positions()
+    ff, _, _, _, _ = O.eng_forces(pos, types_of(s), s.side, SB, SS)
+    noise = O.eng_gauss3(s.seed, np.arange(s.n), 0).astype(np.float32)
+    L = O.oracle_lib()
+    mob = np.array([np.float32(1) / np.float32(SB), np.float32(1) / np.float32(SS)], np.float32)
+    amp = np.array([L.or_eng_amplitude(0.7, float(mob[0]), np.float32(s.dt)),
+                    L.or_eng_amplitude(0.7, float(mob[1]), np.float32(s.dt))], np.float32)
+    ohi, olo, odsp = pos.copy(), np.zeros_like(pos), np.zeros(pos.shape, np.float64)
+    L.or_eng_update(s.n, ohi, olo, odsp, ff, types_of(s), s.side, s.dt, mob, amp, np.ascontiguousarray(noise))
+    d = np.abs(hi - ohi)
+    d = np.minimum(d, s.side - d)
+    assert d.max() < 2e-5, d.max()
+
+
+def test_list_batched_equals_plain_and_graph_equals_single_steps():
+    specs = [(300, 300, 0.5, 1), (1000, 700, 0.55, 2), (150, 450, 0.45, 3)]
+    systems, poss = zip(*[system(*sp, T0=1.0) for sp in specs])
+    eb = B.Engine(list(systems), neighbor_skin=SKIN)
+    eb.set_positions(np.concatenate(poss))
+    eb.run(250)
+    pb, rb = eb.get_positions()
+    for k, (s, p) in enumerate(zip(systems, poss)):
+        e1 = B.Engine([s], neighbor_skin=SKIN)
+        e1.set_positions(p)
+        for _ in range(5):
+            e1.run(50)
+        p1, r1 = e1.get_positions()
+        sl = slice(eb.offsets[k], eb.offsets[k + 1])
+        np.testing.assert_array_equal(pb[sl], p1)
+        np.testing.assert_array_equal(rb[sl], r1)
+    e2 = B.Engine(list(systems), neighbor_skin=SKIN)
+    e2.set_positions(np.concatenate(poss))
+    for _ in range(250):
+        e2.run(1)
+    np.testing.assert_array_equal(e2.get_positions()[0], pb)
+
+
+def test_list_observables_match_oracle():
+    s, pos = system(1200, 1800, 0.5, 8, T0=0.5)
+    e = B.Engine([s], neighbor_skin=SKIN)
+    e.set_positions(pos)
+    e.run(120)
+    ob = e.observe()[0]
+    hi, raw = e.get_positions()
+    _, pot, vir, _, _ = O.eng_forces(hi, types_of(s), s.side, SB, SS)
+    assert ob["energy_big"] == pytest.approx(0.5 * pot[:s.n_big].astype(np.float64).sum() / s.n_big, rel=1e-5)
+    assert ob["virial"] == pytest.approx(vir.astype(np.float64).sum(), rel=1e-5)
+    d = raw[: s.n_big].astype(np.float64) - pos[: s.n_big]
+    assert ob["msd_big"] == pytest.approx((d ** 2).sum(1).mean(), rel=1e-4)
+    counts = e.gder(100, 4.0)[0]
+    p = O.setup_params(s.side, s.n_big, s.n_sml, SB, SS, nbins=100, rng=4.0)
+    np.testing.assert_array_equal(counts, O.gder_counts(p, hi[: s.n_big], hi[s.n_big:]))

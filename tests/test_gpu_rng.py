@@ -74,13 +74,13 @@ def test_rannew64_plain_persistent_and_batched_agree():
                                 T0=1.0, protocol="const"))
     pos = np.concatenate(poss)
     out = []
-    for kw in (dict(), dict(mode="persistent", cluster=2)):
+    for kw in (dict(neighbor_skin=0.0), dict(mode="persistent", cluster=2)):
         e = B.Engine(systems, rng="rannew64", **kw)
         e.set_positions(pos)
         e.run(130)
         out.append(e.get_positions()[0])
     np.testing.assert_array_equal(out[0], out[1])
-    e1 = B.Engine([systems[1]], rng="rannew64")
+    e1 = B.Engine([systems[1]], rng="rannew64", neighbor_skin=0.0)
     e1.set_positions(poss[1])
     e1.run(130)
     np.testing.assert_array_equal(e1.get_positions()[0], out[0][systems[0].n:])
