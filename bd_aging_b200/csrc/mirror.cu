@@ -295,6 +295,66 @@ static int disp_reduce(int kind, const float *raw, const float *r0, int n, float
     return BD_OK;
 }
 
+
+// ------------------------------------------------------------ colours
+// calculate_color / between (colors.cu:8-110) for every big particle, one
+// thread each, in the reference's float operation order (rounding
+// intrinsics: no contraction).  ids: 0 blue, 1 green, 2 red.
+__device__ __forceinline__ bool between_dev(const float3 r1, const float3 r2, const float3 *__restrict__ rs, int ns,
+                                            float side, float side_inv, float max_big, float max_line) {
+    float ux = min_image_f(__fsub_rn(r1.x, r2.x), side, side_inv);
+    float uy = min_image_f(__fsub_rn(r1.y, r2.y), side, side_inv);
+    float uz = min_image_f(__fsub_rn(r1.z, r2.z), side, side_inv);
+    const float ua = __fsqrt_rn(dist2_rn(ux, uy, uz));
+    ux = __fdiv_rn(ux, ua);
+    uy = __fdiv_rn(uy, ua);
+    uz = __fdiv_rn(uz, ua);
+    for (int i = 0; i < ns; i++) {
+        const float3 r = rs[i];
+        const float ax = min_image_f(__fsub_rn(r.x, r1.x), side, side_inv);
+        const float ay = min_image_f(__fsub_rn(r.y, r1.y), side, side_inv);
+        const float az = min_image_f(__fsub_rn(r.z, r1.z), side, side_inv);
+        if (__fsqrt_rn(dist2_rn(ax, ay, az)) > max_big) continue;
+        const float bx = min_image_f(__fsub_rn(r.x, r2.x), side, side_inv);
+        const float by = min_image_f(__fsub_rn(r.y, r2.y), side, side_inv);
+        const float bz = min_image_f(__fsub_rn(r.z, r2.z), side, side_inv);
+        if (__fsqrt_rn(dist2_rn(bx, by, bz)) > max_big) continue;
+        const float cx = __fsub_rn(__fmul_rn(ay, uz), __fmul_rn(az, uy));
+        const float cy = __fadd_rn(__fmul_rn(-ax, uz), __fmul_rn(az, ux));
+        const float cz = __fsub_rn(__fmul_rn(ax, uy), __fmul_rn(ay, ux));
+        if (__fsqrt_rn(dist2_rn(cx, cy, cz)) > max_line) continue;
+        return true;
+    }
+    return false;
+}
+
+__global__ void k_colors(const float3 *__restrict__ rb, int nb, const float3 *__restrict__ rs, int ns, float side,
+                         float sigma_big, float sigma_sml, int *ids, unsigned *counts) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= nb) return;
+    const float side_inv_c = __double2float_rn(1.0 / (double)side);  // calculate_color: 1.0 / side
+    const float side_inv_b = __fdiv_rn(1.0f, side);                  // between: 1 / side
+    const float max_big = __double2float_rn(0.5 * (double)sigma_big + 2.0 * (double)sigma_sml);
+    const float max_line = __double2float_rn(0.35 * (double)sigma_big);
+    const double near2 = (double)sigma_big + 2.0 * (double)sigma_sml;
+    const float3 rm = rb[m];
+    int cid = 0;
+    bool near = false;
+    for (int n = 0; n < nb; n++) {
+        if (n == m) continue;
+        const float3 rn = rb[n];
+        const float dx = min_image_f(__fsub_rn(rn.x, rm.x), side, side_inv_c);
+        const float dy = min_image_f(__fsub_rn(rn.y, rm.y), side, side_inv_c);
+        const float dz = min_image_f(__fsub_rn(rn.z, rm.z), side, side_inv_c);
+        if ((double)dist2_rn(dx, dy, dz) > near2) continue;  // squared distance against a length, as written
+        cid += between_dev(rm, rn, rs, ns, side, side_inv_b, max_big, max_line) ? 1 : -1;
+        near = true;
+    }
+    const int id = near ? (cid > 0 ? 2 : 1) : 0;
+    if (ids) ids[m] = id;
+    atomicAdd(&counts[id], 1u);
+}
+
 }  // namespace bd
 
 using namespace bd;
@@ -555,6 +615,32 @@ int bd_fself_isotropic(const float *rr_raw, const float *rr0, int ngrain, float 
     int rc = disp_reduce(0, rr_raw, rr0, ngrain, qmax, &sum, as_stream(stream));
     if (rc) return rc;
     fself_host[sample_number] += (float)(sum / ngrain);
+    return BD_OK;
+}
+
+int bd_color_statistics(const float *rr_big, const float *rr_sml, int *color_ids, int *counts_host,
+                        const bd_parametros *p, void *stream) {
+    if (!p || !counts_host || p->ngrain_big < 0 || p->ngrain_sml < 0) return BD_ERR_ARG;
+    counts_host[0] = counts_host[1] = counts_host[2] = 0;
+    const int nb = p->ngrain_big, ns = p->ngrain_sml;
+    if (nb == 0) return BD_OK;
+    if (!rr_big || (ns > 0 && !rr_sml)) return BD_ERR_ARG;
+    cudaStream_t s = as_stream(stream);
+    unsigned *d_counts = nullptr;
+    BD_CUDA_TRY(cudaMalloc(&d_counts, 3 * sizeof(unsigned)));
+    cudaError_t ce = cudaMemsetAsync(d_counts, 0, 3 * sizeof(unsigned), s);
+    if (ce == cudaSuccess) {
+        k_colors<<<div_up(nb, 128), 128, 0, s>>>(reinterpret_cast<const float3 *>(rr_big), nb,
+                                                 reinterpret_cast<const float3 *>(rr_sml), ns, p->side,
+                                                 p->sigma_big, p->sigma_sml, color_ids, d_counts);
+        ce = cudaGetLastError();
+    }
+    unsigned h[3] = {0, 0, 0};
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(h, d_counts, sizeof(h), cudaMemcpyDeviceToHost, s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    cudaFree(d_counts);
+    if (ce != cudaSuccess) return BD_ERR_CUDA;
+    for (int k = 0; k < 3; k++) counts_host[k] = (int)h[k];
     return BD_OK;
 }
 

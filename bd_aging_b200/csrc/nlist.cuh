@@ -25,7 +25,7 @@ namespace bd {
 
 constexpr int kMaxNbr = 64;
 #ifndef BD_LIST_GATHER
-#define BD_LIST_GATHER 8  // list partners whose positions are in flight together
+#define BD_LIST_GATHER 4  // list partners whose positions are in flight together
 #endif
 
 struct ListArgs {

@@ -118,6 +118,7 @@ def _lib():
                                    C.c_int, _vp], C.c_int),
             "bd_fself_isotropic": ([_vp, _vp, C.c_int, _vp, C.c_int, C.c_float, _vp], C.c_int),
             "bd_msd": ([_vp, _vp, C.c_int, _vp, _vp], C.c_int),
+            "bd_color_statistics": ([_vp, _vp, _vp, _vp, C.POINTER(Parametros), _vp], C.c_int),
             "bd_cv3d_create": ([C.c_int, C.c_float, C.POINTER(_vp)], C.c_int),
             "bd_cv3d_add_statistics": ([_vp, _vp, _vp, C.c_int, C.c_float, _vp], C.c_int),
             "bd_cv3d_calculate_vector": ([_vp], C.c_int),
@@ -281,6 +282,16 @@ def msd(rr_raw, rr0, ngrain, stream=None) -> float:
     out = np.zeros(1, np.float32)
     _check(_lib().bd_msd(_ptr(rr_raw), _ptr(rr0), ngrain, _ptr(out), _stream(stream)), "msd")
     return float(out[0])
+
+
+def color_statistics(rr_big, rr_sml, pars: Parametros, color_ids=None, stream=None):
+    """calculate_color (colors.cu) for every big particle: device positions in,
+    optional device int ids out (0 blue, 1 green, 2 red); returns the counts
+    (blue, green, red)."""
+    counts = np.zeros(3, np.int32)
+    _check(_lib().bd_color_statistics(_ptr(rr_big), _ptr(rr_sml), _ptr(color_ids), _ptr(counts), C.byref(pars),
+                                      _stream(stream)), "color_statistics")
+    return counts
 
 
 class Contracting_Vector3D:

@@ -176,6 +176,13 @@ int bd_fself_isotropic_noalloc(const float *rr_raw, const float *rr0, int ngrain
 
 /* Mean squared displacement of main.cu:776-792 for one species: returns
  * (1/N) sum |rr_raw - rr0|^2 in *msd_host.  Stream-synchronous. */
+/* calculate_color (colors.cu:64-110) for every big particle, as the snapshot
+ * pass of main.cu:663-713 does (compiled in with GRO_FLAG): colour ids
+ * (device, ngrain_big ints, or NULL) 0 blue (no big neighbour), 1 green,
+ * 2 red (more neighbour pairs with a small particle between them than
+ * without); counts_host[3] = blue, green, red (color_statistics.out). */
+int bd_color_statistics(const float *rr_big, const float *rr_sml, int *color_ids, int *counts_host,
+                        const bd_parametros *p, void *stream);
 int bd_msd(const float *rr_raw, const float *rr0, int ngrain, float *msd_host, void *stream);
 
 /* ---- Contracting_Vector3D (Contracting_Vector3D.cuh:39-75) --------------- */

@@ -713,3 +713,58 @@ int or_precision_run(int mode, int n, int n_big, const float *pos0, double side,
     free(pos); free(ff); free(pot); free(vir); free(dsp); free(rr); free(raw);
     return 0;
 }
+
+/* ------------------------------------------------------------------------
+ * Colour statistics of the snapshot writer (colors.cu:8-110, main.cu:
+ * 663-713): a big particle is Blue without big neighbours (squared distance
+ * compared with sigma_b + 2 sigma_s, as written), else Red when more of its
+ * neighbour pairs have a small particle "between" them than not, else Green.
+ * Float arithmetic in the reference's order; ids: 0 blue, 1 green, 2 red. */
+static float min_image_ref(float d, float side, float side_inv) { return d - side * floorf(side_inv * d + 0.5f); }
+
+static int between_ref(const float *r1, const float *r2, const float *rs, int ns, float side, float sigma_big,
+                       float sigma_sml) {
+    float max_big = (float)(0.5 * sigma_big + 2.0 * sigma_sml);
+    float max_line = (float)(0.35 * sigma_big);
+    float side_inv = 1 / side;
+    float u[3];
+    for (int k = 0; k < 3; k++) u[k] = min_image_ref(r1[k] - r2[k], side, side_inv);
+    float ua = sqrtf(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    for (int k = 0; k < 3; k++) u[k] /= ua;
+    for (int i = 0; i < ns; i++) {
+        const float *r = rs + 3 * i;
+        float d1[3], d2[3];
+        for (int k = 0; k < 3; k++) d1[k] = min_image_ref(r[k] - r1[k], side, side_inv);
+        float n1 = sqrtf(d1[0] * d1[0] + d1[1] * d1[1] + d1[2] * d1[2]);
+        if (n1 > max_big) continue;
+        for (int k = 0; k < 3; k++) d2[k] = min_image_ref(r[k] - r2[k], side, side_inv);
+        float n2 = sqrtf(d2[0] * d2[0] + d2[1] * d2[1] + d2[2] * d2[2]);
+        if (n2 > max_big) continue;
+        float cx = d1[1] * u[2] - d1[2] * u[1], cy = -d1[0] * u[2] + d1[2] * u[0], cz = d1[0] * u[1] - d1[1] * u[0];
+        float dl = sqrtf(cx * cx + cy * cy + cz * cz);
+        if (dl > max_line) continue;
+        return 1;
+    }
+    return 0;
+}
+
+void or_ref_colors(int nb, int ns, const float *rb, const float *rs, float side, float sigma_big, float sigma_sml,
+                   int *ids, int counts[3]) {
+    float side_inv = (float)(1.0 / side);
+    counts[0] = counts[1] = counts[2] = 0;
+    for (int m = 0; m < nb; m++) {
+        int cid = 0, near = 0;
+        for (int n = 0; n < nb; n++) {
+            if (n == m) continue;
+            float d[3];
+            for (int k = 0; k < 3; k++) d[k] = min_image_ref(rb[3 * n + k] - rb[3 * m + k], side, side_inv);
+            float dist = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+            if (dist > sigma_big + 2.0 * sigma_sml) continue;
+            between_ref(rb + 3 * m, rb + 3 * n, rs, ns, side, sigma_big, sigma_sml) ? cid++ : cid--;
+            near = 1;
+        }
+        int id = near ? (cid > 0 ? 2 : 1) : 0;
+        ids[m] = id;
+        counts[id]++;
+    }
+}

@@ -81,6 +81,7 @@ def oracle_lib():
         L.or_ref_sampling_indexes.restype = C.c_int
         L.or_rannew64_next.restype = C.c_double
         L.or_rannew64_particle_noise.argtypes = [C.c_longlong, C.c_int, C.c_int, _f32p]
+        L.or_ref_colors.argtypes = [C.c_int, C.c_int, _f32p, _f32p, C.c_float, C.c_float, C.c_float, _i32p, _i32p]
         L.or_precision_run.argtypes = [C.c_int, C.c_int, C.c_int, _f32p, C.c_double, C.c_double, C.c_double,
                                        C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64, C.c_uint32,
                                        C.c_longlong, C.c_int, C.c_double, _f64p, _f64p]
@@ -123,6 +124,27 @@ def precision_run(mode, pos, n_big, side, sig_big, sig_sml, mob_big, mob_sml, dt
     if rc:
         raise MemoryError("or_precision_run")
     return dict(zip(PRECISION_FIELDS, obs)), dsp
+
+
+def colors(rb, rs, side, sigma_big, sigma_sml):
+    """Colour ids (0 blue, 1 green, 2 red) of the big particles and the
+    blue/green/red counts: restatement of colors.cu."""
+    rb = np.ascontiguousarray(rb, np.float32)
+    rs = np.ascontiguousarray(rs, np.float32)
+    ids = np.zeros(len(rb), np.int32)
+    counts = np.zeros(3, np.int32)
+    oracle_lib().or_ref_colors(len(rb), len(rs), rb, rs, side, sigma_big, sigma_sml, ids, counts)
+    return ids, counts
+
+
+def ref_colors(rb, rs, p: Parametros):
+    """The reference's own calculate_color over every big particle."""
+    L = ref_lib()
+    rb = np.ascontiguousarray(rb, np.float32)
+    rs = np.ascontiguousarray(rs, np.float32)
+    counts = np.zeros(3, np.int32)
+    ids = np.array([L.ref_calculate_color(m, rb, rs, counts, C.byref(p)) for m in range(len(rb))], np.int32)
+    return ids, counts
 
 
 def ref_available() -> bool:
@@ -169,6 +191,8 @@ def ref_lib():
         L.ref_hst_run.argtypes = [P] + [_f32p] * 10 + [_i32p] * 4 + [C.c_long, C.c_long] + [C.c_float] * 4 + \
             [C.c_double, C.c_ulong]
         L.ref_hst_run.restype = C.c_int
+        L.ref_calculate_color.argtypes = [C.c_int, _f32p, _f32p, _i32p, P]
+        L.ref_calculate_color.restype = C.c_int
         _ref = L
     return _ref
 

@@ -3,7 +3,7 @@
 // Test infrastructure: it lets the tests and the golden-vector script call
 // the reference implementation itself (cell_locate_hst, get_forces_*_hst,
 // update_ermak_hst, get_gder_hst, fself_isotropic, calculate_temp_*,
-// sampling_indexes, Contracting_Vector3D) on chosen inputs.
+// sampling_indexes, Contracting_Vector3D, calculate_color) on chosen inputs.
 #include "encabezados.h"
 #include "Contracting_Vector3D.cuh"
 #include <vector>
@@ -66,6 +66,13 @@ void ref_cv3d_add_statistics(void *h, float *rr, float *xx, int n, float side) {
 void ref_cv3d_calculate_vector(void *h) { ((Contracting_Vector3D *)h)->calculate_vector(); }
 void ref_cv3d_get_vector(void *h, float *out) { ((Contracting_Vector3D *)h)->get_vector(out); }
 void ref_cv3d_destroy(void *h) { delete (Contracting_Vector3D *)h; }
+// calculate_color (colors.cu:64-110) of big particle mm: 0 blue, 1 green, 2 red;
+// counts[0..2] = blue, green, red accumulate as in the reference
+int ref_calculate_color(int mm, float *rr_big, float *rr_sml, int *counts, const parametros *p) {
+    char color[20];
+    calculate_color(mm, (float3 *)rr_big, (float3 *)rr_sml, color, counts[0], counts[1], counts[2], *p);
+    return color[0] == 'R' ? 2 : (color[0] == 'G' ? 1 : 0);
+}
 
 }  // extern "C"
 
