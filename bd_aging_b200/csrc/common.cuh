@@ -51,6 +51,70 @@ __device__ __forceinline__ float dist2_rn(float dx, float dy, float dz) {
     return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
 }
 
+// ------------------------------------------------------------------ other potentials
+// Pair potentials of potentials.cu that the reference defines but never
+// calls, for the engine's per-replica potential choice.  pair_extra returns
+// the force factor g (force on the home particle = g (r_partner - r_home))
+// and adds the pair energy to *u.  di = 1/r, sg = the pair's sigma.
+enum PotKind { kPotWcaModified = 0, kPotWca = 1, kPotWca4950 = 2, kPotAO = 3, kPotHsay = 4 };
+
+__device__ __forceinline__ float pair_extra(int pot, const float *pp, float sg, float di, float *u) {
+    const float sor = di * sg;
+    if (pot == kPotWca) {  // potential_wca (potentials.cu:124-135), the +1 outside epsilon as written
+        float s6 = sor * sor * sor;
+        s6 = s6 * s6;
+        const float s12 = s6 * s6;
+        *u += 4.0f * (s12 - s6) + 1.0f;
+        return -4.0f * (12.0f * s12 - 6.0f * s6) * di * di;
+    }
+    const float ros_ao = __double2float_rn(1.0 / (double)sor);  // potentials.cu:102: ros = 1.0 / sor
+    if (pot == kPotWca4950 || (pot == kPotAO && ros_ao <= 1.0f)) {
+        // potential_wca49_50 (potentials.cu:83-95); the AO core (ros <= 1) is the same
+        const float invT = pp[0], AA = pp[1];
+        const float s6 = sor * sor * sor * sor * sor * sor;
+        const float s12 = s6 * s6, s24 = s12 * s12, s48 = s24 * s24;
+        const float s50 = s48 * sor * sor;
+        *u += AA * invT * (s50 - s48 * sor) + invT;
+        return -AA * invT * (50.0f * s50 - 49.0f * s48 * sor) * di * di;
+    }
+    if (pot == kPotAO) {  // depletion branch of potential_wca49_50_AO (potentials.cu:97-122)
+        const float sigma_pol = pp[2], phi_pol = pp[3];
+        const float size_ratio = sg / sigma_pol;
+        const float ros = ros_ao;
+        const float ros3 = ros * ros * ros;
+        const float eta1 = size_ratio + 1.0f, eta2 = eta1 * eta1;
+        *u += -phi_pol * (eta2 * eta1 - 1.5f * eta2 * ros + 0.5f * ros3);
+        return phi_pol * (1.5f * eta2 * ros - 1.5f * ros3) * di * di;
+    }
+    // kPotHsay: hard-sphere core (40-20) plus attractive Yukawa tail,
+    // U = [(s/r)^40 - 2 (s/r)^20 + 1]_{r<s} - (s/r) exp(-z (r/s - 1)), written
+    // as potential_hsay (potentials.cu:149-176) intends: ros = r / s, energies
+    // added, g = (dU/dr) / r
+    const float z = pp[0];
+    const float ros = 1.0f / sor;
+    float dudr = 0.f;
+    if (ros < 1.0f) {
+        const float s2 = sor * sor, s4 = s2 * s2, s8 = s4 * s4, s16 = s8 * s8;
+        const float s20 = s4 * s16, s40 = s20 * s20;
+        *u += s40 - 2.0f * s20 + 1.0f;
+        dudr += -40.0f * (s40 - s20) * di;
+    }
+    const float uatt = -sor * expf(-z * (ros - 1.0f));
+    *u += uatt;
+    dudr -= (1.0f + ros * z) * uatt * di;
+    return dudr * di;
+}
+// cut distance of a pair in units of its sigma
+__host__ __device__ inline float pot_cut_factor(int pot, const float *pp, float sg) {
+    switch (pot) {
+        case kPotWca: return 1.12246205f;        // 2^(1/6): the minimum of 4 (s^12 - s^6)
+        case kPotWca4950: return 50.0f / 49.0f;  // the minimum of s^50 - s^49
+        case kPotAO: return 1.0f + sg / pp[2];   // the depletion term vanishes at r = s (1 + s / sigma_pol)
+        case kPotHsay: return pp[1];             // Yukawa tail truncated at pp[1] sigma
+        default: return 1.0f;                    // get_forces.cu:331-334
+    }
+}
+
 // ------------------------------------------------------------------ rannew64
 // rannew64 (rannew64.cu:55-126): subtractive lagged Fibonacci x[np] -= x[nq]
 // over a 250-word ring (taps 250 and 103, pointers walking down from 249 and

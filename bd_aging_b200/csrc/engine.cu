@@ -470,10 +470,19 @@ int setup_geometry(bd_engine *e) {
         S.sig[0] = d.sigma_big;
         S.sig[1] = 0.5f * (d.sigma_big + d.sigma_sml);  // get_forces.cu:441
         S.sig[2] = d.sigma_sml;
-        for (int k = 0; k < 3; k++) S.cut2[k] = S.sig[k] * S.sig[k];
-        float rcmax = std::max(S.sig[0], std::max(S.sig[1], S.sig[2]));
+        S.pot = d.potential;
+        for (int k = 0; k < 4; k++) S.pp[k] = d.pot_param[k];
+        if (S.pot < kPotWcaModified || S.pot > kPotHsay) return BD_ERR_ARG;
+        if (S.pot == kPotAO && !(S.pp[2] > 0.f)) return BD_ERR_ARG;
+        if (S.pot == kPotHsay && !(S.pp[1] >= 1.0f && S.pp[1] <= 4.0f)) return BD_ERR_ARG;
+        float cut[3];
+        for (int k = 0; k < 3; k++) {
+            cut[k] = S.pot == kPotWcaModified ? S.sig[k] : S.sig[k] * pot_cut_factor(S.pot, S.pp, S.sig[k]);
+            S.cut2[k] = cut[k] * cut[k];
+        }
+        float rcmax = std::max(cut[0], std::max(cut[1], cut[2]));
         const float skin = e->list ? e->skin : 0.f;  // list builds sweep cut + skin
-        for (int k = 0; k < 3; k++) S.lcut2[k] = (S.sig[k] + skin) * (S.sig[k] + skin);
+        for (int k = 0; k < 3; k++) S.lcut2[k] = (cut[k] + skin) * (cut[k] + skin);
         S.skin_half2 = 0.25f * skin * skin;
         int nc = (int)std::floor((double)d.side / ((double)(rcmax + skin) * (1.0 + 1e-5)));
         if (nc < 3) return BD_ERR_ARG;  // box too small for a 27-cell sweep

@@ -36,6 +36,8 @@ struct SysDev {
     float T0, Tf, t0, tf, period;
     unsigned long long seed;
     int nbx, nby, nbz, brick_base;
+    int pot;           // PotKind
+    float pp[4];       // potential parameters
     float lcut2[3];    // neighbour-list mode: (cut distance + skin)^2 per species pair
     float skin_half2;  //   (skin / 2)^2: a particle farther than this from its build position
 };

@@ -229,11 +229,17 @@ __global__ void __launch_bounds__(256) k_step_list(ListArgs a, const long long *
             if (d2 < (tj ? c1 : c0)) {
                 const float sg = tj ? sg1 : sg0;
                 const float di = rsqrtf(d2);
-                const float sor = di * sg;
-                const float s2 = sor * sor;
-                const float s6 = s2 * s2 * s2;
-                const float s12 = s6 * s6;
-                const float g = -12.0f * (s12 - s6) * (di * di);
+                float g;
+                if (S.pot == kPotWcaModified) {
+                    const float sor = di * sg;
+                    const float s2 = sor * sor;
+                    const float s6 = s2 * s2 * s2;
+                    const float s12 = s6 * s6;
+                    g = -12.0f * (s12 - s6) * (di * di);
+                } else {
+                    float u = 0.f;
+                    g = pair_extra(S.pot, S.pp, sg, di, &u);
+                }
                 fx = fmaf(g, dx, fx);
                 fy = fmaf(g, dy, fy);
                 fz = fmaf(g, dz, fz);

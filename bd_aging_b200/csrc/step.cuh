@@ -127,7 +127,7 @@ struct PairSums {
 template <bool OBS, bool CENSUS>
 __device__ __forceinline__ void flush_queue(const BrickSmem &sm, const StepArgs &a, int nq, float mx, float my,
                                             float mz, int tm, float L, float sgbb, float sgbs, float sgss,
-                                            int part_base, PairSums &ps) {
+                                            int part_base, int pot, const float *pp, PairSums &ps) {
     const int T = blockDim.x, tid = threadIdx.x;
     for (int e = 0; e < nq; e++) {
         const int j = sm.queue[e * T + tid];
@@ -138,18 +138,25 @@ __device__ __forceinline__ void flush_queue(const BrickSmem &sm, const StepArgs 
         const float d2 = dist2_rn(dx, dy, dz);
         const int pt = tm + (int)(tcj & 1u);
         const float sg = pt == 0 ? sgbb : (pt == 1 ? sgbs : sgss);
-        // WCA-modified pair (potentials.cu:137-147) in terms of 1/r
+        // WCA-modified pair (potentials.cu:137-147) in terms of 1/r, or the
+        // replica's other potential
         const float di = rsqrtf(d2);
-        const float sor = di * sg;
-        const float s2 = sor * sor;
-        const float s6 = s2 * s2 * s2;
-        const float s12 = s6 * s6;
-        const float g = -12.0f * (s12 - s6) * (di * di);  // pair force = g d
+        float g, u = 0.f;
+        if (pot == kPotWcaModified) {
+            const float sor = di * sg;
+            const float s2 = sor * sor;
+            const float s6 = s2 * s2 * s2;
+            const float s12 = s6 * s6;
+            g = -12.0f * (s12 - s6) * (di * di);  // pair force = g d
+            u = s12 - 2.0f * s6 + 1.0f;
+        } else {
+            g = pair_extra(pot, pp, sg, di, &u);
+        }
         ps.fx = fmaf(g, dx, ps.fx);
         ps.fy = fmaf(g, dy, ps.fy);
         ps.fz = fmaf(g, dz, ps.fz);
         if (OBS) {
-            ps.pot += s12 - 2.0f * s6 + 1.0f;
+            ps.pot += u;
             ps.vir = fmaf(-0.5f * g, d2, ps.vir);
         }
         if (CENSUS) {
@@ -316,7 +323,7 @@ __device__ void process_brick(const StepArgs &a, int bidx, long long ni, unsigne
                 const int hr = h - 1 + hx * (dy + hy * dz);  // row of 3 contiguous halo cells
                 const int j0 = sm.start[hr], j1 = sm.start[hr + 3];
                 if (nq + (j1 - j0) > kQueue) {
-                    flush_queue<OBS, CENSUS>(sm, a, nq, mx, my, mz, tm, L, sgbb, sgbs, sgss, part_base, ps);
+                    flush_queue<OBS, CENSUS>(sm, a, nq, mx, my, mz, tm, L, sgbb, sgbs, sgss, part_base, S.pot, S.pp, ps);
                     nq = 0;
                 }
                 const bool wrap =
@@ -326,7 +333,7 @@ __device__ void process_brick(const StepArgs &a, int bidx, long long ni, unsigne
                 else
                     sweep_row<false>(sm, view, j0, j1, si, wrap, mx, my, mz, mxx, myy, mzz, L, nq);
             }
-        flush_queue<OBS, CENSUS>(sm, a, nq, mx, my, mz, tm, L, sgbb, sgbs, sgss, part_base, ps);
+        flush_queue<OBS, CENSUS>(sm, a, nq, mx, my, mz, tm, L, sgbb, sgbs, sgss, part_base, S.pot, S.pp, ps);
         float fx = ps.fx, fy = ps.fy, fz = ps.fz;
         if (S.fcap > 0.f) {  // capped forces for the initial relaxation
             const float fmx = fmaxf(fabsf(fx), fmaxf(fabsf(fy), fabsf(fz)));

@@ -23,6 +23,7 @@ BD_ERR_TIMEOUT, BD_ERR_FILE, BD_ERR_FORMAT, BD_ERR_NUMERIC = 6, 7, 8, 9
 STATUS_NAMES = {0: "BD_OK", 1: "BD_ERR_ARG", 2: "BD_ERR_CUDA", 3: "BD_ERR_CELL_OVERFLOW", 4: "BD_ERR_NOMEM",
                 5: "BD_ERR_STATE", 6: "BD_ERR_TIMEOUT", 7: "BD_ERR_FILE", 8: "BD_ERR_FORMAT", 9: "BD_ERR_NUMERIC"}
 PROTOCOL = {"linear": 0, "sine": 1, "const": 2}
+POTENTIAL = {"wca_modified": 0, "wca": 1, "wca49_50": 2, "ao": 3, "hsay": 4}
 RNG = {"philox": 0, "curand": 1, "noise": 2, "rannew64": 3}
 MODE = {"auto": 0, "plain": 1, "persistent": 2}
 GDER = {"auto": 0, "all_pairs": 1, "cells": 2}
@@ -51,7 +52,8 @@ class SystemDesc(C.Structure):
     _fields_ = [("n_big", C.c_int), ("n_sml", C.c_int), ("side", C.c_float), ("sigma_big", C.c_float),
                 ("sigma_sml", C.c_float), ("mob_big", C.c_float), ("mob_sml", C.c_float), ("dt", C.c_double),
                 ("temp_protocol", C.c_int), ("T0", C.c_float), ("Tf", C.c_float), ("t0", C.c_float),
-                ("tf", C.c_float), ("period", C.c_float), ("seed", C.c_ulonglong), ("force_cap", C.c_float)]
+                ("tf", C.c_float), ("period", C.c_float), ("seed", C.c_ulonglong), ("force_cap", C.c_float),
+                ("potential", C.c_int), ("pot_param", C.c_float * 4)]
 
 
 class EngineOpts(C.Structure):
@@ -340,6 +342,8 @@ class System:
     seed: int = 1
     mobility: str = "reference"   # "reference": 1/sigma; "unit": D0 = 1
     force_cap: float = 0.0
+    potential: str = "wca_modified"  # POTENTIAL keys; parameters in pot_param (bd_aging.h BD_POT_*)
+    pot_param: tuple = (0.0, 0.0, 0.0, 0.0)
 
     def desc(self) -> SystemDesc:
         d = SystemDesc()
@@ -355,6 +359,9 @@ class System:
         d.T0, d.Tf, d.t0, d.tf, d.period = self.T0, self.Tf, self.t0, self.tf, self.period
         d.seed = self.seed
         d.force_cap = self.force_cap
+        d.potential = POTENTIAL[self.potential]
+        for k in range(4):
+            d.pot_param[k] = float(self.pot_param[k]) if k < len(self.pot_param) else 0.0
         return d
 
     @property

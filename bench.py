@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--replicas", type=int, default=64)
     ap.add_argument("--md-steps", type=int, default=960)
     ap.add_argument("--no-extras", action="store_true", help="skip plain/e2e/reference-CUDA/CPU legs")
+    ap.add_argument("--only-leg", default=None, choices=["correlator", "gder"],
+                    help="after the timed steps run only this extra leg (for profiling)")
     ap.add_argument("--brick", type=int, nargs=3, default=None, help="cells per brick (default: engine's)")
     ap.add_argument("--threads", type=int, default=0, help="CTA size (default: engine's)")
     ap.add_argument("--relax-steps", type=int, default=2000,
@@ -260,6 +262,24 @@ def reference_cuda(steps=200):
             "ms_per_step": ms.value / steps}
 
 
+def gder_leg(eng, systems, nbins=400, rng=15.0, iters=3):
+    """g(r) counts of every replica (bd_engine_gder, exact integers; the
+    reference scripts' 400 bins to r = 15, run-fself.sh:46-47).  Work =
+    ordered pairs tested: N^2 per replica on the all-pairs path, or the
+    candidates of the cell stencil."""
+    import torch
+    eng.gder(nbins, rng)
+    st = torch.cuda.ExternalStream(eng.stream_handle())
+    t0 = time.perf_counter()
+    for _ in range(iters):
+        eng.gder(nbins, rng)
+    st.synchronize()
+    t = (time.perf_counter() - t0) / iters
+    pairs = float(sum(s.n * (s.n - 1) for s in systems))
+    return {"ms_per_call": t * 1e3, "nbins": nbins, "range": rng, "ordered_pairs": pairs,
+            "pair_evaluations_per_s": pairs / t, "note": "wall time of the call (exact u64 counts copied back)"}
+
+
 def correlator_leg(eng, P, slots=16, iters=20, q=6.19):
     """Waiting-time correlator on the bench batch: `slots` displacement
     snapshots, then all of them reduced against the current state in one
@@ -442,7 +462,12 @@ def run_ours(args):
                          "alg_bytes_per_launch": ALG_BYTES_PER_PARTICLE_STEP * P,
                          "traffic": (tpp * P) if tpp else None},
             "clocks": ck}
-    if rank == 0 and world == 1 and not args.no_extras:
+    if rank == 0 and world == 1 and args.only_leg:
+        if args.only_leg == "correlator":
+            line["correlator"] = correlator_leg(eng, P)
+        else:
+            line["gder"] = gder_leg(eng, systems)
+    elif rank == 0 and world == 1 and not args.no_extras:
         # plain single-replica engine, same system
         s1 = systems[0]
         e1 = B.Engine([s1], graph_steps=96, brick=args.brick, threads=args.threads, neighbor_skin=args.skin)
@@ -473,6 +498,7 @@ def run_ours(args):
         except Exception as ex:  # reported, never fatal for the bench line
             line["reference_cuda"] = {"error": str(ex)[:200]}
         line["cpu_baseline"] = cpu_baseline()
+        line["gder"] = gder_leg(eng, systems)
         line["correlator"] = correlator_leg(eng, P)
         eng.close()
         line["precision"] = precision_leg()

@@ -240,7 +240,23 @@ typedef struct bd_system_desc {
     float T0, Tf, t0, tf, period;
     unsigned long long seed;   /* RNG key of this replica (idum for BD_RNG_CURAND) */
     float force_cap;           /* > 0: |F| capped (initial-configuration relaxation) */
+    int potential;             /* BD_POT_* (0: the reference's modified WCA) */
+    float pot_param[4];        /* parameters of the potential, see BD_POT_* */
 } bd_system_desc;
+
+/* Pair potentials (potentials.cu).  The reference's step uses the modified
+ * WCA only (get_forces.cu); the others are defined there and never called.
+ * Cut distances are per species pair, in units of the pair's sigma s. */
+#define BD_POT_WCA_MODIFIED 0  /* (s/r)^12 - 2 (s/r)^6 + 1, cut s (potentials.cu:137-147) */
+#define BD_POT_WCA 1           /* 4 ((s/r)^12 - (s/r)^6) + 1, cut 2^(1/6) s (potentials.cu:124-135) */
+#define BD_POT_WCA49_50 2      /* A invT ((s/r)^50 - (s/r)^49) + invT, cut 50/49 s; pot_param = {invT, A}
+                                  (potentials.cu:83-95) */
+#define BD_POT_AO 3            /* 49-50 core for r <= s, Asakura-Oosawa depletion beyond, cut
+                                  s (1 + s / sigma_pol); pot_param = {invT, A, sigma_pol, phi_pol}
+                                  (potentials.cu:97-122) */
+#define BD_POT_HSAY 4          /* 40-20 core for r < s plus -(s/r) exp(-z (r/s - 1)), cut c s;
+                                  pot_param = {z, c}.  potentials.cu:149-176 writes ros = s r, assigns
+                                  the energy and flips the core force; this is its evident intent */
 
 typedef struct bd_engine_opts {
     int rng;                   /* BD_RNG_* */

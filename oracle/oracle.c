@@ -768,3 +768,97 @@ void or_ref_colors(int nb, int ns, const float *rb, const float *rs, float side,
         counts[id]++;
     }
 }
+
+/* ------------------------------------------------------------------------
+ * Pair potentials of potentials.cu that the reference never calls (host
+ * float formulas as written, EPS = 1): *pot accumulates, *nf = normal force
+ * (dU/dr).  pot: 1 wca, 2 wca49_50, 3 AO, 4 HSAY (the intended form: ros = r/s,
+ * energies added, dU/dr).  pp = {invT, AA, sigma_pol, phi_pol} or {z, cut}. */
+void or_pair_extra(int pot, const float *pp, float sigma, float dist_inv, float *u, float *nf) {
+    float sor = dist_inv * sigma;
+    if (pot == 1) {
+        float s6 = sor * sor * sor;
+        s6 = s6 * s6;
+        float s12 = s6 * s6;
+        *u += 4 * (s12 - s6) + 1;
+        *nf = -4 * (12 * s12 - 6 * s6) * dist_inv;
+        return;
+    }
+    float ros_ao = (float)(1.0 / sor);
+    if (pot == 2 || (pot == 3 && ros_ao <= 1.0)) {
+        float invT = pp[0], AA = pp[1];
+        float s6;
+        if (pot == 2) {  /* potential_wca49_50_hst: (s^3)^2 */
+            s6 = sor * sor * sor;
+            s6 = s6 * s6;
+        } else {         /* potential_wca49_50_AO_hst: s s s s s s */
+            s6 = sor * sor * sor * sor * sor * sor;
+        }
+        float s12 = s6 * s6, s24 = s12 * s12, s48 = s24 * s24, s50 = s48 * sor * sor;
+        *u += AA * invT * (s50 - s48 * sor) + invT;
+        *nf = -AA * invT * (50 * s50 - 49 * s48 * sor) * dist_inv;
+        return;
+    }
+    if (pot == 3) {
+        float size_ratio = sigma / pp[2], phi_pol = pp[3];
+        float ros = ros_ao, ros3 = ros * ros * ros;
+        float eta1 = (float)(size_ratio + 1.0), eta2 = eta1 * eta1;
+        /* double literals: the bracket, the product and the sum are double */
+        double val = (double)(-1.0f * phi_pol) * (((double)(eta2 * eta1) - 1.5 * eta2 * ros) + 0.5 * ros3);
+        *u = (float)((double)*u + val);
+        *nf = (float)((double)(1.0f * phi_pol) * (1.5 * eta2 * ros - 1.5 * ros3) * dist_inv);
+        return;
+    }
+    /* 4: HSAY as intended */
+    float z = pp[0], ros = 1.0f / sor, dudr = 0.0f;
+    if (ros < 1.0f) {
+        float s2 = sor * sor, s4 = s2 * s2, s8 = s4 * s4, s16 = s8 * s8, s20 = s4 * s16, s40 = s20 * s20;
+        *u += s40 - 2.0f * s20 + 1.0f;
+        dudr += -40.0f * (s40 - s20) * dist_inv;
+    }
+    float uatt = -sor * expf(-z * (ros - 1.0f));
+    *u += uatt;
+    dudr -= (1.0f + ros * z) * uatt * dist_inv;
+    *nf = dudr;
+}
+
+/* Engine forces with a potential of potentials.cu (all pairs, index order,
+ * the engine's cut distances): as or_eng_forces, pair arithmetic from
+ * or_pair_extra (pot 0: the modified WCA). */
+void or_eng_forces_pot(int n, const float *pos, const int *type, float side, const float sigma[2], int pot,
+                       const float *pp, float *ff, float *potv, float *vir) {
+    float side_inv = 1.0f / side;
+    float sg[2][2];
+    sg[0][0] = sigma[0]; sg[1][1] = sigma[1];
+    sg[0][1] = sg[1][0] = 0.5f * (sigma[0] + sigma[1]);
+    for (int m = 0; m < n; m++) {
+        float fx = 0, fy = 0, fz = 0, pm = 0, vm = 0;
+        for (int j = 0; j < n; j++) {
+            if (j == m) continue;
+            float s = sg[type[m]][type[j]], c;
+            switch (pot) {
+                case 1: c = s * 1.12246205f; break;
+                case 2: c = s * (50.0f / 49.0f); break;
+                case 3: c = s * (1.0f + s / pp[2]); break;
+                case 4: c = s * pp[1]; break;
+                default: c = s;
+            }
+            float dx = pos[3 * j] - pos[3 * m], dy = pos[3 * j + 1] - pos[3 * m + 1], dz = pos[3 * j + 2] - pos[3 * m + 2];
+            dx -= side * floorf(side_inv * dx + 0.5f);
+            dy -= side * floorf(side_inv * dy + 0.5f);
+            dz -= side * floorf(side_inv * dz + 0.5f);
+            float d2 = dx * dx + dy * dy + dz * dz;
+            if (d2 < c * c) {
+                float di = sqrtf(1.0f / d2), nf;
+                if (pot == 0) wca_modified(s, di, &pm, &nf);
+                else or_pair_extra(pot, pp, s, di, &pm, &nf);
+                float px = nf * di * dx, py = nf * di * dy, pz = nf * di * dz;
+                fx += px; fy += py; fz += pz;
+                vm -= 0.5f * (dx * px + dy * py + dz * pz);
+            }
+        }
+        ff[3 * m] = fx; ff[3 * m + 1] = fy; ff[3 * m + 2] = fz;
+        if (potv) potv[m] = pm;
+        if (vir) vir[m] = vm;
+    }
+}

@@ -82,6 +82,8 @@ def oracle_lib():
         L.or_rannew64_next.restype = C.c_double
         L.or_rannew64_particle_noise.argtypes = [C.c_longlong, C.c_int, C.c_int, _f32p]
         L.or_ref_colors.argtypes = [C.c_int, C.c_int, _f32p, _f32p, C.c_float, C.c_float, C.c_float, _i32p, _i32p]
+        L.or_pair_extra.argtypes = [C.c_int, _f32p, C.c_float, C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        L.or_eng_forces_pot.argtypes = [C.c_int, _f32p, _i32p, C.c_float, _f32p, C.c_int, _f32p, _f32p, _f32p, _f32p]
         L.or_precision_run.argtypes = [C.c_int, C.c_int, C.c_int, _f32p, C.c_double, C.c_double, C.c_double,
                                        C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64, C.c_uint32,
                                        C.c_longlong, C.c_int, C.c_double, _f64p, _f64p]
@@ -147,6 +149,28 @@ def ref_colors(rb, rs, p: Parametros):
     return ids, counts
 
 
+POT = {"wca_modified": 0, "wca": 1, "wca49_50": 2, "ao": 3, "hsay": 4}
+
+
+def pair_extra(pot, pp, sigma, dist_inv):
+    """(energy, normal force) of one pair with a potential of potentials.cu."""
+    u, nf = C.c_float(0), C.c_float(0)
+    oracle_lib().or_pair_extra(POT[pot], np.ascontiguousarray(pp, np.float32), sigma, dist_inv, C.byref(u),
+                               C.byref(nf))
+    return u.value, nf.value
+
+
+def eng_forces_pot(pos, types, side, sigma_big, sigma_sml, pot, pp):
+    n = len(pos)
+    ff = np.zeros((n, 3), np.float32)
+    potv = np.zeros(n, np.float32)
+    vir = np.zeros(n, np.float32)
+    oracle_lib().or_eng_forces_pot(n, np.ascontiguousarray(pos, np.float32), np.ascontiguousarray(types, np.int32),
+                                   side, np.array([sigma_big, sigma_sml], np.float32), POT[pot],
+                                   np.ascontiguousarray(pp, np.float32), ff, potv, vir)
+    return ff, potv, vir
+
+
 def ref_available() -> bool:
     return os.path.exists(LIB_REF)
 
@@ -192,6 +216,11 @@ def ref_lib():
             [C.c_double, C.c_ulong]
         L.ref_hst_run.restype = C.c_int
         L.ref_calculate_color.argtypes = [C.c_int, _f32p, _f32p, _i32p, P]
+        F = C.c_float
+        FP = C.POINTER(C.c_float)
+        L.ref_potential_wca_hst.argtypes = [F, F, FP, FP]
+        L.ref_potential_wca49_50_hst.argtypes = [F, F, F, F, FP, FP]
+        L.ref_potential_wca49_50_AO_hst.argtypes = [F, F, F, F, F, F, FP, FP]
         L.ref_calculate_color.restype = C.c_int
         _ref = L
     return _ref

@@ -66,6 +66,17 @@ void ref_cv3d_add_statistics(void *h, float *rr, float *xx, int n, float side) {
 void ref_cv3d_calculate_vector(void *h) { ((Contracting_Vector3D *)h)->calculate_vector(); }
 void ref_cv3d_get_vector(void *h, float *out) { ((Contracting_Vector3D *)h)->get_vector(out); }
 void ref_cv3d_destroy(void *h) { delete (Contracting_Vector3D *)h; }
+// the host potentials of potentials.cu that the reference never calls
+void ref_potential_wca_hst(float sigma, float dist_inv, float *pot, float *nf) {
+    potential_wca_hst(sigma, dist_inv, *pot, *nf);
+}
+void ref_potential_wca49_50_hst(float sigma, float dist_inv, float invT, float AA, float *pot, float *nf) {
+    potential_wca49_50_hst(sigma, dist_inv, invT, AA, *pot, *nf);
+}
+void ref_potential_wca49_50_AO_hst(float sigma, float dist_inv, float invT, float AA, float sigma_pol, float phi_pol,
+                                   float *pot, float *nf) {
+    potential_wca49_50_AO_hst(sigma, dist_inv, invT, AA, sigma_pol, phi_pol, *pot, *nf);
+}
 // calculate_color (colors.cu:64-110) of big particle mm: 0 blue, 1 green, 2 red;
 // counts[0..2] = blue, green, red accumulate as in the reference
 int ref_calculate_color(int mm, float *rr_big, float *rr_sml, int *counts, const parametros *p) {

@@ -1,0 +1,75 @@
+"""The engine with the other pair potentials of potentials.cu (standard WCA,
+WCA 49-50, 49-50 + Asakura-Oosawa depletion, HSAY): energies and virial
+against the oracle's all-pairs forces, one injected-noise step against the
+oracle update (sweep path), and the list path against the sweep path."""
+import numpy as np
+import pytest
+
+from bd_aging_b200 import configs as CF
+from bd_aging_b200 import lib as B
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+SB, SS = float(CF.SIGMA_BIG), float(CF.SIGMA_SML)
+CASES = [("wca", (0, 0, 0, 0)), ("wca49_50", (1.4, 0.8, 0, 0)), ("ao", (1.0, 0.9, 2.0, 0.2)),
+         ("hsay", (2.0, 2.0, 0, 0))]
+
+
+def system(pot, pp, nb=1500, ns=1500, phi=0.45, seed=3, **kw):
+    side = float(np.float32(CF.side_from_phi(nb, ns, phi)))
+    pos = CF.lattice_config(nb, ns, side, seed)
+    s = B.System(n_big=nb, n_sml=ns, side=side, sigma_big=SB, sigma_sml=SS, dt=1e-5, seed=seed, T0=0.5,
+                 protocol="const", potential=pot, pot_param=pp, **kw)
+    return s, pos
+
+
+def types_of(s):
+    return np.array([0] * s.n_big + [1] * s.n_sml, np.int32)
+
+
+@pytest.mark.parametrize("pot,pp", CASES)
+def test_energy_and_virial_match_oracle(pot, pp):
+    s, pos = system(pot, pp)
+    e = B.Engine([s])
+    e.set_positions(pos)
+    ob = e.observe()[0]
+    _, u, vir = O.eng_forces_pot(pos, types_of(s), s.side, SB, SS, pot, pp)
+    u = u.astype(np.float64)
+    assert ob["energy_big"] == pytest.approx(0.5 * u[:s.n_big].sum() / s.n_big, rel=1e-4, abs=1e-6)
+    assert ob["energy_sml"] == pytest.approx(0.5 * u[s.n_big:].sum() / s.n_sml, rel=1e-4, abs=1e-6)
+    assert ob["virial"] == pytest.approx(vir.astype(np.float64).sum(), rel=1e-4, abs=1e-3)
+
+
+@pytest.mark.parametrize("pot,pp", CASES)
+def test_injected_noise_step_matches_oracle(pot, pp):
+    s, pos = system(pot, pp)
+    e = B.Engine([s], rng="noise")
+    e.set_positions(pos)
+    noise = np.random.default_rng(2).standard_normal((s.n, 3)).astype(np.float32)
+    e.set_noise(noise)
+    e.run(1)
+    hi, _ = e.get_positions()
+    ff, _, _ = O.eng_forces_pot(pos, types_of(s), s.side, SB, SS, pot, pp)
+    L = O.oracle_lib()
+    mob = np.array([np.float32(1) / np.float32(SB), np.float32(1) / np.float32(SS)], np.float32)
+    amp = np.array([L.or_eng_amplitude(0.5, float(mob[0]), np.float32(s.dt)),
+                    L.or_eng_amplitude(0.5, float(mob[1]), np.float32(s.dt))], np.float32)
+    ohi, olo, odsp = pos.copy(), np.zeros_like(pos), np.zeros(pos.shape, np.float64)
+    L.or_eng_update(s.n, ohi, olo, odsp, ff, types_of(s), s.side, s.dt, mob, amp, noise)
+    d = np.abs(hi - ohi)
+    d = np.minimum(d, s.side - d)
+    assert d.max() < 5e-6, d.max()
+
+
+@pytest.mark.parametrize("pot,pp", CASES)
+def test_list_path_tracks_sweep_path(pot, pp):
+    s, pos = system(pot, pp, force_cap=100.0)  # the 49-50 cores are stiff on a lattice start
+    out = []
+    for skin in (0.0, 0.25):
+        e = B.Engine([s], neighbor_skin=skin)
+        e.set_positions(pos)
+        e.run(50)
+        out.append(e.get_positions()[0])
+    d = np.abs(out[0] - out[1])
+    d = np.minimum(d, s.side - d)
+    assert d.max() < 1e-4, d.max()
