@@ -284,7 +284,10 @@ int list_rebuild(bd_engine *e, int cur) {
 }
 template <int RNG>
 int launch_list_step_t(bd_engine *e, const ListArgs &a, int ni_off) {
-    k_step_list<RNG><<<div_up(e->P, 256), 256, 0, e->stream>>>(a, e->d_ni, ni_off);
+    if (e->extra_pot)
+        k_step_list<RNG, true><<<div_up(e->P, BD_LIST_THREADS), BD_LIST_THREADS, 0, e->stream>>>(a, e->d_ni, ni_off);
+    else
+        k_step_list<RNG, false><<<div_up(e->P, BD_LIST_THREADS), BD_LIST_THREADS, 0, e->stream>>>(a, e->d_ni, ni_off);
     BD_LAUNCH_CHECK();
     return BD_OK;
 }
@@ -471,6 +474,7 @@ int setup_geometry(bd_engine *e) {
         S.sig[1] = 0.5f * (d.sigma_big + d.sigma_sml);  // get_forces.cu:441
         S.sig[2] = d.sigma_sml;
         S.pot = d.potential;
+        if (d.potential != kPotWcaModified) e->extra_pot = true;
         for (int k = 0; k < 4; k++) S.pp[k] = d.pot_param[k];
         if (S.pot < kPotWcaModified || S.pot > kPotHsay) return BD_ERR_ARG;
         if (S.pot == kPotAO && !(S.pp[2] > 0.f)) return BD_ERR_ARG;
@@ -565,6 +569,17 @@ int bd_engine_create(const bd_system_desc *systems, int nsys, const bd_engine_op
         rc = setup_geometry(e);
     }
     if (rc) { delete e; return rc; }
+    if (opts.cell_capacity <= 0) {
+        // default capacity: room for twice the densest replica's mean cell
+        // occupancy plus 8 (long cut distances make large cells)
+        double occ = 0.0;
+        for (const SysDev &S : e->sysh) occ = std::max(occ, (double)S.n / ((double)S.ncell * S.ncell * S.ncell));
+        const int want = std::min(kQueue / 3, (int)std::ceil(2.0 * occ + 8.0));
+        if (want > e->cap) {
+            e->cap = want;
+            if ((rc = setup_geometry(e))) { delete e; return rc; }
+        }
+    }
 #define ALLOC(ptr, bytes)                                                    \
     do {                                                                     \
         if (cudaMalloc((void **)&(ptr), (bytes)) != cudaSuccess) {          \

@@ -70,6 +70,7 @@ struct bd_engine {
     // neighbour-list mode (plain mode with generated noise): positions by
     // storage id (double-buffered, e->cur selects), build positions, lists
     bool list = false;
+    bool extra_pot = false;  // some replica uses a potential other than the modified WCA
     float skin = 0.f;
     float4 *lpos[2] = {nullptr, nullptr};
     float4 *pbuild = nullptr;

@@ -27,6 +27,12 @@ constexpr int kMaxNbr = 64;
 #ifndef BD_LIST_GATHER
 #define BD_LIST_GATHER 4  // list partners whose positions are in flight together
 #endif
+#ifndef BD_LIST_THREADS
+#define BD_LIST_THREADS 256  // CTA size of the list step
+#endif
+#ifndef BD_LIST_MINB
+#define BD_LIST_MINB 4       // resident CTAs per SM asked of the register allocator (64 registers)
+#endif
 
 struct ListArgs {
     const SysDev *sys;
@@ -182,8 +188,11 @@ __global__ void k_list_done(int *flag, int nrep, long long *builds) {
 // One time step of every particle from its list (thread per storage id).
 // Force sum in list order; update, compensated position and FP64
 // displacement exactly as process_brick.
-template <int RNG>
-__global__ void __launch_bounds__(256) k_step_list(ListArgs a, const long long *ni_base, int ni_off) {
+// EXTRA: some replica of the batch uses a potential other than the modified
+// WCA (instantiated separately so the default kernel keeps its registers).
+template <int RNG, bool EXTRA>
+__global__ void __launch_bounds__(BD_LIST_THREADS, BD_LIST_MINB) k_step_list(ListArgs a, const long long *ni_base,
+                                                                          int ni_off) {
     const int sid = blockIdx.x * blockDim.x + threadIdx.x;
     if (sid >= a.np) return;
     const long long ni = *ni_base + ni_off;
@@ -230,7 +239,7 @@ __global__ void __launch_bounds__(256) k_step_list(ListArgs a, const long long *
                 const float sg = tj ? sg1 : sg0;
                 const float di = rsqrtf(d2);
                 float g;
-                if (S.pot == kPotWcaModified) {
+                if (!EXTRA || S.pot == kPotWcaModified) {
                     const float sor = di * sg;
                     const float s2 = sor * sor;
                     const float s6 = s2 * s2 * s2;

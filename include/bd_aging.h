@@ -260,7 +260,8 @@ typedef struct bd_system_desc {
 
 typedef struct bd_engine_opts {
     int rng;                   /* BD_RNG_* */
-    int cell_capacity;         /* slots per cell (0 = 16, 24 in list mode; at most 24) */
+    int cell_capacity;         /* slots per cell, at most 24 (0: 16, or 24 in list mode, or more
+                                  when the cells hold more than 4 particles on average) */
     int brick[3];              /* cells per brick (0 = autotune / default) */
     int threads;               /* CTA size (0 = default) */
     int mode;                  /* BD_MODE_* */

@@ -111,3 +111,30 @@ def test_list_observables_match_oracle():
     counts = e.gder(100, 4.0)[0]
     p = O.setup_params(s.side, s.n_big, s.n_sml, SB, SS, nbins=100, rng=4.0)
     np.testing.assert_array_equal(counts, O.gder_counts(p, hi[: s.n_big], hi[s.n_big:]))
+
+
+def test_single_species_replicas_in_a_batch():
+    specs = [(0, 800, 0.45, 41), (600, 0, 0.45, 42), (300, 300, 0.5, 43)]
+    systems, poss = zip(*[system(*sp, T0=0.8) for sp in specs])
+    e = B.Engine(list(systems))
+    e.set_positions(np.concatenate(poss))
+    e.reserve_snapshots(1)
+    e.snapshot(0)
+    e.run(200)
+    obs = e.observe()
+    c = e.correlate([0], 6.19)[0]
+    hi, _ = e.get_positions()
+    cnt, hsh = e.census()
+    for k, s in enumerate(systems):
+        sl = slice(e.offsets[k], e.offsets[k + 1])
+        _, _, _, nbr, h = O.eng_forces(hi[sl], types_of(s), s.side, SB, SS)
+        np.testing.assert_array_equal(cnt[sl], nbr)
+        np.testing.assert_array_equal(hsh[sl], h)
+        o = obs[k]
+        assert all(np.isfinite(v) for v in o.values())
+        if s.n_big == 0:
+            assert o["msd_big"] == 0.0 and o["energy_big"] == 0.0 and c[k]["msd_big"] == 0.0
+            assert c[k]["msd_sml"] > 0.0
+        if s.n_sml == 0:
+            assert o["msd_sml"] == 0.0 and c[k]["fself_sml"] == 0.0
+            assert c[k]["msd_big"] > 0.0

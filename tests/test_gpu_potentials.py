@@ -12,12 +12,29 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 SB, SS = float(CF.SIGMA_BIG), float(CF.SIGMA_SML)
 CASES = [("wca", (0, 0, 0, 0)), ("wca49_50", (1.4, 0.8, 0, 0)), ("ao", (1.0, 0.9, 2.0, 0.2)),
-         ("hsay", (2.0, 2.0, 0, 0))]
+         ("hsay", (2.0, 1.6, 0, 0))]
+_RELAXED = {}
 
 
-def system(pot, pp, nb=1500, ns=1500, phi=0.45, seed=3, **kw):
+def relaxed(nb, ns, side, seed):
+    """Lattice start relaxed by capped modified-WCA steps: no core overlaps, so
+    the stiff 49-50 cores give moderate forces."""
+    key = (nb, ns, side, seed)
+    if key not in _RELAXED:
+        s = B.System(n_big=nb, n_sml=ns, side=side, sigma_big=SB, sigma_sml=SS, dt=1e-4, seed=seed, T0=0.2,
+                     protocol="const", force_cap=100.0)
+        e = B.Engine([s], rng_stream=1)
+        e.set_positions(CF.lattice_config(nb, ns, side, seed))
+        e.run(600)
+        _RELAXED[key] = e.get_positions()[0]
+        e.close()
+    return _RELAXED[key].copy()
+
+
+def system(pot, pp, nb=1500, ns=1500, phi=0.3, seed=3, **kw):
+    # phi = 0.3: the long AO / HSAY cut distances make large cells (capacity 24)
     side = float(np.float32(CF.side_from_phi(nb, ns, phi)))
-    pos = CF.lattice_config(nb, ns, side, seed)
+    pos = relaxed(nb, ns, side, seed)
     s = B.System(n_big=nb, n_sml=ns, side=side, sigma_big=SB, sigma_sml=SS, dt=1e-5, seed=seed, T0=0.5,
                  protocol="const", potential=pot, pot_param=pp, **kw)
     return s, pos
@@ -63,7 +80,7 @@ def test_injected_noise_step_matches_oracle(pot, pp):
 
 @pytest.mark.parametrize("pot,pp", CASES)
 def test_list_path_tracks_sweep_path(pot, pp):
-    s, pos = system(pot, pp, force_cap=100.0)  # the 49-50 cores are stiff on a lattice start
+    s, pos = system(pot, pp)
     out = []
     for skin in (0.0, 0.25):
         e = B.Engine([s], neighbor_skin=skin)
