@@ -27,6 +27,9 @@ constexpr int kMaxNbr = 64;
 #ifndef BD_LIST_GATHER
 #define BD_LIST_GATHER 4  // list partners whose positions are in flight together
 #endif
+#ifndef BD_LIST_PIPE
+#define BD_LIST_PIPE 1       // load the next chunk's list words under this chunk's gathers
+#endif
 #ifndef BD_LIST_THREADS
 #define BD_LIST_THREADS 256  // CTA size of the list step
 #endif
@@ -213,20 +216,28 @@ __global__ void __launch_bounds__(BD_LIST_THREADS, BD_LIST_MINB) k_step_list(Lis
     // partners in chunks of kGather: all list words, then all positions in
     // flight, then the pair arithmetic in list order
     constexpr int kGather = BD_LIST_GATHER;
+    // the list words of the next chunk load while this chunk's positions do
+    int jn[kGather];
+#pragma unroll
+    for (int u = 0; u < kGather; u++) jn[u] = (u < n) ? __ldg(a.nbr + (size_t)u * a.np + sid) : -1;
     for (int k0 = 0; k0 < n; k0 += kGather) {
         int jj[kGather];
         float4 pj[kGather];
 #pragma unroll
         for (int u = 0; u < kGather; u++) {
-            jj[u] = (k0 + u < n) ? __ldg(a.nbr + (size_t)(k0 + u) * a.np + sid) : -1;
-        }
-#pragma unroll
-        for (int u = 0; u < kGather; u++) {
+            jj[u] = jn[u];
             const bool ok = (unsigned)jj[u] < (unsigned)a.np;
             if (jj[u] >= 0 && !ok) set_status(a.status, kStatArg);  // never true for consistent lists
             pj[u] = ok ? __ldg(a.pos_in + jj[u]) : make_float4(0.f, 0.f, 0.f, 0.f);
             if (!ok) jj[u] = -1;
         }
+#if BD_LIST_PIPE
+#pragma unroll
+        for (int u = 0; u < kGather; u++) {
+            const int k = k0 + kGather + u;
+            jn[u] = (k < n) ? __ldg(a.nbr + (size_t)k * a.np + sid) : -1;
+        }
+#endif
 #pragma unroll
         for (int u = 0; u < kGather; u++) {
             if (jj[u] < 0) continue;
@@ -254,6 +265,13 @@ __global__ void __launch_bounds__(BD_LIST_THREADS, BD_LIST_MINB) k_step_list(Lis
                 fz = fmaf(g, dz, fz);
             }
         }
+#if !BD_LIST_PIPE
+#pragma unroll
+        for (int u = 0; u < kGather; u++) {
+            const int k = k0 + kGather + u;
+            jn[u] = (k < n) ? __ldg(a.nbr + (size_t)k * a.np + sid) : -1;
+        }
+#endif
     }
     if (S.fcap > 0.f) {  // capped forces for the initial relaxation
         const float fmx = fmaxf(fabsf(fx), fmaxf(fabsf(fy), fabsf(fz)));

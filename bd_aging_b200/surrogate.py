@@ -251,3 +251,36 @@ def crossing_study(phi=0.52, tw=100, lag=3000, k=7.0, budget=6, seeds=(1, 2, 3, 
     return {"t_star": t_star, "grid": t_grid, "surrogate": t_sur, "err_grid": abs(t_grid - t_star),
             "err_surrogate": abs(t_sur - t_star), "proposals": proposals, "budget": budget,
             "f_truth": [float(v) for v in f_truth], "ts_truth": [float(v) for v in ts_truth]}
+
+
+# ------------------------------------------------------------------ held-out error
+TRAIN_TW = (10, 100, 300, 1000)                      # steps at dt = 1e-4
+TRAIN_LAGS = tuple(int(v) for v in np.unique(np.geomspace(10, 3000, 12).astype(int)))
+TRAIN_KS = (5.0, 6.0, 7.0, 8.0, 9.0)
+
+
+def build_dataset(phis, temps, seeds, t_ws=TRAIN_TW, lags=TRAIN_LAGS, ks=TRAIN_KS, n_per_replica=1000,
+                  dt=1e-4, seed=1):
+    """Training rows from one batched run: every (phi, T_final) x seed is a
+    replica; each contributes one row per (t_w, lag, k)."""
+    settings = [(float(p), float(t)) for p in phis for t in temps for _ in range(seeds)]
+    return simulate(settings, list(t_ws), list(lags), list(ks), n_per_replica=n_per_replica, dt=dt, seed=seed)
+
+
+def seed_average(X, Y):
+    """Rows with identical inputs (replicas of one setting) averaged."""
+    keys, inv = np.unique(np.round(X.astype(np.float64), 6), axis=0, return_inverse=True)
+    inv = inv.ravel()
+    ys = np.zeros((len(keys), Y.shape[1]))
+    np.add.at(ys, inv, Y)
+    cnt = np.bincount(inv, minlength=len(keys))[:, None]
+    return keys.astype(np.float32), (ys / cnt).astype(np.float32)
+
+
+def held_out_fs_error(model, phis, temps, seeds=4, n_per_replica=1000, dt=1e-4, seed=777):
+    """Mean and max |F_s(predicted) - F_s(simulated)| over plain runs at
+    settings the model has not seen (seed-averaged simulations)."""
+    X, Y = build_dataset(phis, temps, seeds, n_per_replica=n_per_replica, dt=dt, seed=seed)
+    Xa, Ya = seed_average(X, Y)
+    err = np.abs(model.predict(Xa)[:, 0] - Ya[:, 0])
+    return float(err.mean()), float(err.max()), len(Xa)

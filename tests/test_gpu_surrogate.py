@@ -84,3 +84,17 @@ def test_proposals_beat_a_uniform_grid():
     assert 0.05 < r["t_star"] < 1.0, r
     assert r["err_surrogate"] < r["err_grid"], r
     assert r["err_surrogate"] < 0.05, r
+
+
+def test_held_out_fs_error_below_0_02():
+    """Trained on engine runs over a (phi, T_final) grid, the surrogate
+    predicts F_s of plain runs at unseen settings within 0.02 on average."""
+    from bd_aging_b200 import surrogate as S
+    X, Y = S.build_dataset(phis=(0.50, 0.55, 0.60), temps=np.linspace(0.05, 1.0, 8), seeds=8)
+    assert len(X) > 40000
+    model = S.SurrogateModel(seed=3)
+    model.fit(X, Y, steps=4000, lr=1e-3)
+    mean_err, max_err, n = S.held_out_fs_error(model, phis=(0.525, 0.575), temps=(0.2, 0.45, 0.7, 0.9))
+    model.close()
+    assert n > 100
+    assert mean_err < 0.02, (mean_err, max_err)
