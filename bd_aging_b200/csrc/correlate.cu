@@ -42,7 +42,9 @@ __global__ void __launch_bounds__(kCorrThreads) k_corr_partial(const int2 *__res
                                                                const double *__restrict__ dz,
                                                                const double *__restrict__ snaps, long long P,
                                                                SlotList sl, double q, double *__restrict__ part) {
-    __shared__ double red[kCorrThreads / 32][kCorrFields];
+    // per-warp partial sums of every slot; one barrier, then a fixed-order
+    // reduction over the warps
+    __shared__ double red[kMaxCorrSlots][kCorrThreads / 32][kCorrFields];
     const int2 sg = segs[blockIdx.x];  // (replica, first storage id)
     const SysDev &S = sys[sg.x];
     const int end = min(sg.y + kCorrChunk, S.part_base + S.n);
@@ -64,6 +66,7 @@ __global__ void __launch_bounds__(kCorrThreads) k_corr_partial(const int2 *__res
         }
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll 2
     for (int j = 0; j < sl.n; j++) {
         const double *bx = snaps + (size_t)sl.slot[j] * 3 * (size_t)P;
         const double *by = bx + P, *bz = by + P;
@@ -87,16 +90,16 @@ __global__ void __launch_bounds__(kCorrThreads) k_corr_partial(const int2 *__res
             double v = acc[f];
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-            if (lane == 0) red[warp][f] = v;
+            if (lane == 0) red[j][warp][f] = v;
         }
-        __syncthreads();
-        if (threadIdx.x < kCorrFields) {
-            double v = 0.0;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < sl.n * kCorrFields; t += kCorrThreads) {
+        const int j = t / kCorrFields, f = t % kCorrFields;
+        double v = 0.0;
 #pragma unroll
-            for (int w = 0; w < kCorrThreads / 32; w++) v += red[w][threadIdx.x];
-            part[((size_t)blockIdx.x * sl.n + j) * kCorrFields + threadIdx.x] = v;
-        }
-        __syncthreads();
+        for (int w = 0; w < kCorrThreads / 32; w++) v += red[j][w][f];
+        part[((size_t)blockIdx.x * sl.n + j) * kCorrFields + f] = v;
     }
 }
 

@@ -376,6 +376,25 @@ def surrogate_leg(steps=200, warmup=20, batch=4096):
             "gemm_launches_per_step": 14}
 
 
+def surrogate_quality_leg():
+    """The surrogate trained on engine runs (phi in {0.50, 0.55, 0.60} x 8
+    T_final x 8 seeds, 4 waiting times x 12 lags x 5 wave numbers: 46k samples,
+    4000 Adam steps) and its F_s error on plain runs at unseen settings
+    (phi in {0.525, 0.575} x T_final in {0.2, 0.45, 0.7, 0.9}, 4 seeds each)."""
+    from bd_aging_b200 import surrogate as S
+    t0 = time.perf_counter()
+    X, Y = S.build_dataset(phis=(0.50, 0.55, 0.60), temps=np.linspace(0.05, 1.0, 8), seeds=8)
+    t1 = time.perf_counter()
+    model = S.SurrogateModel(seed=3)
+    loss = model.fit(X, Y, steps=4000, lr=1e-3)
+    t2 = time.perf_counter()
+    mean_err, max_err, n = S.held_out_fs_error(model, phis=(0.525, 0.575), temps=(0.2, 0.45, 0.7, 0.9))
+    model.close()
+    return {"train_samples": int(len(X)), "final_loss": loss, "held_out_points": n,
+            "held_out_fs_mean_abs_err": mean_err, "held_out_fs_max_abs_err": max_err,
+            "data_generation_s": t1 - t0, "training_s": t2 - t1}
+
+
 _RELAXED_CACHE = {}
 
 
@@ -503,6 +522,7 @@ def run_ours(args):
         eng.close()
         line["precision"] = precision_leg()
         line["surrogate"] = surrogate_leg()
+        line["surrogate_quality"] = surrogate_quality_leg()
     eng.close()
     ranks.finalize()
     if rank == 0:
