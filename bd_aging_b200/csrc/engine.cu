@@ -263,10 +263,11 @@ int rebuild_grid(bd_engine *e, long long work) {
 // gates the work, `rflag` (per replica, or null for all) selects replicas
 // (e->lflag inside steps; e->d_one and null for observation passes).
 int list_bin(bd_engine *e, int cur, const int *any, const int *rflag) {
-    k_list_clear<<<rebuild_grid(e, div_up(e->C, 256)), 256, 0, e->stream>>>(e->cnt[0], e->C, any);
-    k_list_bin<<<rebuild_grid(e, div_up(e->P, 256)), 256, 0, e->stream>>>(e->lpos[cur & 1], (int)e->P, e->rep_of_sid,
-                                                                        e->d_sys, e->cnt[0], e->pos[0], e->cap,
-                                                                        e->status, any, rflag);
+    cudaStream_t st = e->stream;
+    k_list_clear<<<rebuild_grid(e, div_up(e->C, 256)), 256, 0, st>>>(e->cnt[0], e->C, any);
+    k_list_bin<<<rebuild_grid(e, div_up(e->P, 256)), 256, 0, st>>>(e->lpos[cur & 1], (int)e->P, e->rep_of_sid,
+                                                                 e->d_sys, e->cnt[0], e->pos[0], e->cap, e->status,
+                                                                 any, rflag);
     BD_LAUNCH_CHECK();
     return BD_OK;
 }
@@ -274,11 +275,12 @@ int list_bin(bd_engine *e, int cur, const int *any, const int *rflag) {
 // no replica is flagged).  Rebuild decisions are per replica, so a replica
 // gets the same lists alone as in any batch.
 int list_rebuild(bd_engine *e, int cur) {
+    cudaStream_t st = e->stream;
     int rc = list_bin(e, cur, e->lflag + e->R, e->lflag);
     if (rc) return rc;
     ListBuild lb{e->nbr, e->nnb, e->pbuild, e->lpos[cur & 1], e->lflag, e->R};
-    k_list_build<<<rebuild_grid(e, e->nbricks), e->threads, e->smem, e->stream>>>(make_args(e, 0, 0), lb);
-    k_list_done<<<1, 256, 0, e->stream>>>(e->lflag, e->R, e->d_builds);
+    k_list_build<<<rebuild_grid(e, e->nbricks), e->threads, e->smem, st>>>(make_args(e, 0, 0), lb);
+    k_list_done<<<1, 256, 0, st>>>(e->lflag, e->R, e->d_builds);
     BD_LAUNCH_CHECK();
     return BD_OK;
 }
@@ -291,16 +293,18 @@ int launch_list_step_t(bd_engine *e, const ListArgs &a, int ni_off) {
     BD_LAUNCH_CHECK();
     return BD_OK;
 }
-// one list-mode step in phase `cur`: conditional rebuild, then the step
-int list_step(bd_engine *e, int cur, int ni_off) {
-    int rc = list_rebuild(e, cur);
-    if (rc) return rc;
-    const ListArgs a = make_largs(e, cur);
+int launch_list_step(bd_engine *e, const ListArgs &a, int ni_off) {
     switch (e->rng) {
         case BD_RNG_CURAND: return launch_list_step_t<kRngCurand>(e, a, ni_off);
         case BD_RNG_RANNEW64: return launch_list_step_t<kRngRannew64>(e, a, ni_off);
         default: return launch_list_step_t<kRngPhilox>(e, a, ni_off);
     }
+}
+// one list-mode step in phase `cur`: gated rebuild, then the step
+int list_step(bd_engine *e, int cur, int ni_off) {
+    int rc = list_rebuild(e, cur);
+    if (rc) return rc;
+    return launch_list_step(e, make_largs(e, cur), ni_off);
 }
 // observation passes read cell buckets: rebuild them from the by-id positions
 int sync_buckets(bd_engine *e) { return e->list ? list_bin(e, e->cur, e->d_one, nullptr) : BD_OK; }
@@ -363,7 +367,8 @@ void free_engine(bd_engine *e) {
                     e->rep_of_gid, e->x0, e->obs, e->snap, e->nbr_count, e->nbr_hash, e->cr, e->noise,
                     e->status, e->d_ni, e->out_pos, e->out_raw, e->d_cl_start, e->d_cl_bricks, e->rn_ring, e->rn_lcg,
                     e->snaps, e->d_segs, e->d_seg_first, e->corr_part, e->corr_out, e->lpos[0], e->lpos[1],
-                    e->pbuild, e->nbr, e->nnb, e->lflag, e->d_one, e->d_builds};
+                    e->pbuild, e->nbr, e->nnb, e->lflag, e->d_one, e->d_builds, e->ld_in, e->ld_staged,
+                    e->ld_slot, e->ld_bucket, e->ld_cnt, e->ld_start, e->ld_bsum, e->ld_bad};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -488,6 +493,9 @@ int setup_geometry(bd_engine *e) {
         const float skin = e->list ? e->skin : 0.f;  // list builds sweep cut + skin
         for (int k = 0; k < 3; k++) S.lcut2[k] = (cut[k] + skin) * (cut[k] + skin);
         S.skin_half2 = 0.25f * skin * skin;
+        // list partners are within rcmax + skin at the build and each end has
+        // moved at most skin / 2 since
+        S.interior = rcmax + 2.0f * skin + 0.01f;
         int nc = (int)std::floor((double)d.side / ((double)(rcmax + skin) * (1.0 + 1e-5)));
         if (nc < 3) return BD_ERR_ARG;  // box too small for a 27-cell sweep
         S.ncell = nc;
@@ -619,8 +627,8 @@ int bd_engine_create(const bd_system_desc *systems, int nsys, const bd_engine_op
         ALLOC(e->nnb, sizeof(int) * P);
         ALLOC(e->lflag, sizeof(int) * (e->R + 1));
         ALLOC(e->d_one, sizeof(int));
-        ALLOC(e->d_builds, sizeof(long long));
-        cudaMemsetAsync(e->d_builds, 0, sizeof(long long), e->stream);
+        ALLOC(e->d_builds, 2 * sizeof(long long));
+        cudaMemsetAsync(e->d_builds, 0, 2 * sizeof(long long), e->stream);
         const int one = 1;
         cudaMemcpyAsync(e->d_one, &one, sizeof(int), cudaMemcpyHostToDevice, e->stream);
     }
@@ -677,9 +685,11 @@ int bd_engine_get_info(const bd_engine *e, bd_engine_info *info) {
     info->next_step = e->ni;
     info->neighbor_skin = e->list ? e->skin : 0.f;
     if (e->list) {
-        BD_CUDA_TRY(cudaMemcpyAsync(&info->list_builds, e->d_builds, sizeof(long long), cudaMemcpyDeviceToHost,
-                                    e->stream));
+        long long b[2];
+        BD_CUDA_TRY(cudaMemcpyAsync(b, e->d_builds, sizeof(b), cudaMemcpyDeviceToHost, e->stream));
         BD_CUDA_TRY(cudaStreamSynchronize(e->stream));
+        info->list_builds = b[0];
+        info->list_rebuild_steps = b[1];
     }
     return BD_OK;
 }
@@ -693,53 +703,50 @@ int bd_engine_get_stream(const bd_engine *e, void **stream) {
 int bd_engine_set_positions(bd_engine *e, const float *pos) {
     if (!e || !pos) return BD_ERR_ARG;
     const size_t P = (size_t)e->P;
-    // storage order: replica, brick, cell within brick, reference index
-    std::vector<long long> key(P);
-    std::vector<int> order(P);
-    for (int r = 0; r < e->R; r++) {
-        const SysDev &S = e->sysh[r];
-        for (int i = 0; i < S.n; i++) {
-            size_t g = (size_t)S.part_base + i;
-            float x = pos[3 * g], y = pos[3 * g + 1], z = pos[3 * g + 2];
-            if (!(x >= 0.f && x <= S.L && y >= 0.f && y <= S.L && z >= 0.f && z <= S.L)) return BD_ERR_ARG;
-            int ix = std::min(std::max((int)(x * S.cinv), 0), S.ncell - 1);
-            int iy = std::min(std::max((int)(y * S.cinv), 0), S.ncell - 1);
-            int iz = std::min(std::max((int)(z * S.cinv), 0), S.ncell - 1);
-            long long b = (ix / e->bx) + (long long)S.nbx * ((iy / e->by) + (long long)S.nby * (iz / e->bz));
-            long long c = (ix % e->bx) + e->bx * ((iy % e->by) + e->by * (iz % e->bz));
-            key[g] = (((long long)r << 40) | (b << 16) | c);
-            order[g] = (int)g;
-        }
+    // storage order: replica, brick, cell within brick, reference index --
+    // computed on the device (keys, counting sort over the slots, per-slot
+    // sort by reference index)
+    const long long V = (long long)e->bx * e->by * e->bz, T = (long long)e->nbricks * V;
+    if (T > INT_MAX) return BD_ERR_ARG;
+    if (!e->ld_in) {
+        BD_CUDA_TRY(cudaMalloc(&e->ld_in, sizeof(float) * 3 * P));
+        BD_CUDA_TRY(cudaMalloc(&e->ld_staged, sizeof(float4) * P));
+        BD_CUDA_TRY(cudaMalloc(&e->ld_slot, sizeof(int) * P));
+        BD_CUDA_TRY(cudaMalloc(&e->ld_bucket, sizeof(int) * P));
+        BD_CUDA_TRY(cudaMalloc(&e->ld_bad, sizeof(unsigned)));
     }
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key[a] < key[b]; });
-    std::vector<float4> staged(P);
-    std::vector<int> gid_of(P), rep_of_sid(P);
-    for (size_t sid = 0; sid < P; sid++) {
-        int g = order[sid];
-        int r = 0;
-        // replica of g
-        {
-            int lo = 0, hi = e->R - 1;
-            while (lo < hi) {
-                int mid = (lo + hi + 1) / 2;
-                if (e->sysh[mid].part_base <= g) lo = mid; else hi = mid - 1;
-            }
-            r = lo;
-        }
-        const SysDev &S = e->sysh[r];
-        unsigned type = (g - S.part_base) < S.n_big ? 0u : 1u;
-        unsigned w = (unsigned)sid | (type << 31);
-        float wf;
-        std::memcpy(&wf, &w, 4);
-        staged[sid] = make_float4(pos[3 * (size_t)g], pos[3 * (size_t)g + 1], pos[3 * (size_t)g + 2], wf);
-        gid_of[sid] = g;
-        rep_of_sid[sid] = r;
+    if (T > e->ld_slots) {  // the brick shape sets the slot count
+        if (e->ld_cnt) cudaFree(e->ld_cnt);
+        if (e->ld_start) cudaFree(e->ld_start);
+        if (e->ld_bsum) cudaFree(e->ld_bsum);
+        e->ld_cnt = e->ld_start = e->ld_bsum = nullptr;
+        e->ld_slots = 0;
+        BD_CUDA_TRY(cudaMalloc(&e->ld_cnt, sizeof(int) * T));
+        BD_CUDA_TRY(cudaMalloc(&e->ld_start, sizeof(int) * T));
+        BD_CUDA_TRY(cudaMalloc(&e->ld_bsum, sizeof(int) * (T / kScanBlock + 1)));
+        e->ld_slots = T;
     }
-    float4 *d_staged = nullptr;
-    BD_CUDA_TRY(cudaMalloc(&d_staged, sizeof(float4) * P));
-    cudaMemcpyAsync(d_staged, staged.data(), sizeof(float4) * P, cudaMemcpyHostToDevice, e->stream);
-    cudaMemcpyAsync(e->gid_of, gid_of.data(), sizeof(int) * P, cudaMemcpyHostToDevice, e->stream);
-    cudaMemcpyAsync(e->rep_of_sid, rep_of_sid.data(), sizeof(int) * P, cudaMemcpyHostToDevice, e->stream);
+    const int n = (int)T, nb = (int)div_up(T, kScanBlock);
+    const int gp = rebuild_grid(e, div_up((long long)P, 256)), gt = rebuild_grid(e, div_up(T, 256));
+    BD_CUDA_TRY(cudaMemcpyAsync(e->ld_in, pos, sizeof(float) * 3 * P, cudaMemcpyHostToDevice, e->stream));
+    cudaMemsetAsync(e->ld_cnt, 0, sizeof(int) * T, e->stream);
+    cudaMemsetAsync(e->ld_bad, 0, sizeof(unsigned), e->stream);
+    k_order_keys<<<gp, 256, 0, e->stream>>>(e->ld_in, (int)P, e->rep_of_gid, e->d_sys, e->bx, e->by, e->bz,
+                                            e->ld_slot, e->ld_cnt, e->ld_bad);
+    BD_LAUNCH_CHECK();
+    unsigned bad = 0;
+    BD_CUDA_TRY(cudaMemcpyAsync(&bad, e->ld_bad, sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream));
+    BD_CUDA_TRY(cudaStreamSynchronize(e->stream));
+    if (bad) return BD_ERR_ARG;  // nothing of the engine state has changed
+    int *start = e->ld_start;  // the scan runs on a copy of the counts
+    cudaMemcpyAsync(start, e->ld_cnt, sizeof(int) * T, cudaMemcpyDeviceToDevice, e->stream);
+    k_scan_local<<<nb, kScanThreads, 0, e->stream>>>(start, n, e->ld_bsum);
+    k_scan_totals<<<1, kScanThreads, 0, e->stream>>>(e->ld_bsum, nb);
+    k_scan_add<<<div_up(T, 256), 256, 0, e->stream>>>(start, n, e->ld_bsum);
+    k_order_fill<<<gp, 256, 0, e->stream>>>(e->ld_slot, (int)P, start, e->ld_cnt, e->ld_bucket);
+    k_order_emit<<<gt, 256, 0, e->stream>>>(start, n, (int)P, e->cap, e->ld_bucket, e->ld_in, e->rep_of_gid,
+                                            e->d_sys, e->ld_staged, e->gid_of, e->rep_of_sid);
+    BD_LAUNCH_CHECK();
     for (int k = 0; k < 3; k++) {
         cudaMemsetAsync(e->cnt[k], 0, sizeof(int) * e->C, e->stream);
         cudaMemsetAsync(e->lo[k], 0, sizeof(float) * P, e->stream);
@@ -753,7 +760,7 @@ int bd_engine_set_positions(bd_engine *e, const float *pos) {
         for (int g = 0; g < 3; g++)
             if (e->gexec[g]) { cudaGraphExecDestroy(e->gexec[g]); e->gexec[g] = nullptr; }
     }
-    k_load<<<div_up((long)P, 256), 256, 0, e->stream>>>(d_staged, (int)P, e->rep_of_sid, e->d_sys, e->cnt[0],
+    k_load<<<div_up((long)P, 256), 256, 0, e->stream>>>(e->ld_staged, (int)P, e->rep_of_sid, e->d_sys, e->cnt[0],
                                                         e->pos[0], e->cap, e->x0, e->gid_of, e->status,
                                                         e->list ? e->lpos[0] : nullptr);
     if (e->list) {  // every replica's lists are built before its first step
@@ -765,7 +772,6 @@ int bd_engine_set_positions(bd_engine *e, const float *pos) {
                                                                      e->gid_of, (int)P);
     cudaError_t le = cudaGetLastError();
     cudaStreamSynchronize(e->stream);
-    cudaFree(d_staged);
     if (le != cudaSuccess) return BD_ERR_CUDA;
 
     e->loaded = true;

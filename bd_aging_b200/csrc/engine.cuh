@@ -40,6 +40,8 @@ struct SysDev {
     float pp[4];       // potential parameters
     float lcut2[3];    // neighbour-list mode: (cut distance + skin)^2 per species pair
     float skin_half2;  //   (skin / 2)^2: a particle farther than this from its build position
+    float interior;    //   a particle at least this far from every face has no list partner
+                       //   across the boundary (largest list distance + skin, plus a margin)
 };
 
 // per-replica observation accumulators (FP64)

@@ -111,6 +111,162 @@ namespace bd {
 
 __global__ void k_advance_counter(long long *ni_base, int k) { *ni_base += k; }
 
+// ------------------------------------------------------------- storage order
+// set_positions on the device.  A particle's slot is (replica, brick, cell
+// within the brick) numbered in the order of the brick table; storage ids
+// run over the slots in order and, within a slot, by reference index.
+constexpr int kScanThreads = 1024, kScanPer = 4, kScanBlock = kScanThreads * kScanPer;
+
+// slot of every particle (reference order) and the particle count per slot;
+// a position outside [0, L] (or NaN) sets *bad and gets no slot
+__global__ void k_order_keys(const float *__restrict__ pos3, int P, const int *__restrict__ rep_of_gid,
+                             const SysDev *__restrict__ sys, int bx, int by, int bz, int *__restrict__ slot_of,
+                             int *__restrict__ slot_cnt, unsigned *bad) {
+    const int V = bx * by * bz;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < P; g += gridDim.x * blockDim.x) {
+        const SysDev &S = sys[rep_of_gid[g]];
+        const float x = pos3[3 * (size_t)g], y = pos3[3 * (size_t)g + 1], z = pos3[3 * (size_t)g + 2];
+        if (!(x >= 0.f && x <= S.L && y >= 0.f && y <= S.L && z >= 0.f && z <= S.L)) {
+            atomicOr(bad, 1u);
+            slot_of[g] = -1;
+            continue;
+        }
+        const int nc = S.ncell;
+        const int ix = min(max((int)__fmul_rn(x, S.cinv), 0), nc - 1);
+        const int iy = min(max((int)__fmul_rn(y, S.cinv), 0), nc - 1);
+        const int iz = min(max((int)__fmul_rn(z, S.cinv), 0), nc - 1);
+        const int b = ix / bx + S.nbx * (iy / by + S.nby * (iz / bz));
+        const int c = ix % bx + bx * (iy % by + by * (iz % bz));
+        const int slot = (S.brick_base + b) * V + c;
+        slot_of[g] = slot;
+        atomicAdd(slot_cnt + slot, 1);
+    }
+}
+
+// exclusive scan, pass 1: each block scans kScanBlock entries in place and
+// writes its total
+__global__ void __launch_bounds__(kScanThreads) k_scan_local(int *__restrict__ v, int n, int *__restrict__ bsum) {
+    __shared__ int wsum[kScanThreads / 32];
+    const int base = blockIdx.x * kScanBlock + threadIdx.x * kScanPer;
+    int x[kScanPer], t = 0;
+#pragma unroll
+    for (int i = 0; i < kScanPer; i++) {
+        x[i] = base + i < n ? v[base + i] : 0;
+        t += x[i];
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int inc = t;  // inclusive warp scan of the thread totals
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, inc, off);
+        if (lane >= off) inc += y;
+    }
+    if (lane == 31) wsum[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        int w = lane < kScanThreads / 32 ? wsum[lane] : 0;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, w, off);
+            if (lane >= off) w += y;
+        }
+        wsum[lane] = w;  // inclusive over warps
+    }
+    __syncthreads();
+    int run = inc - t + (warp ? wsum[warp - 1] : 0);
+#pragma unroll
+    for (int i = 0; i < kScanPer; i++) {
+        if (base + i < n) v[base + i] = run;
+        run += x[i];
+    }
+    if (threadIdx.x == kScanThreads - 1) bsum[blockIdx.x] = run;
+}
+// pass 2 (one block): exclusive scan of the block totals
+__global__ void __launch_bounds__(kScanThreads) k_scan_totals(int *bsum, int nb) {
+    __shared__ int carry;
+    __shared__ int wsum[kScanThreads / 32];
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int b0 = 0; b0 < nb; b0 += kScanThreads) {
+        const int i = b0 + threadIdx.x;
+        const int t = i < nb ? bsum[i] : 0;
+        int inc = t;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, inc, off);
+            if (lane >= off) inc += y;
+        }
+        if (lane == 31) wsum[warp] = inc;
+        __syncthreads();
+        if (warp == 0) {
+            int w = wsum[lane];
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, w, off);
+                if (lane >= off) w += y;
+            }
+            wsum[lane] = w;
+        }
+        __syncthreads();
+        const int excl = carry + inc - t + (warp ? wsum[warp - 1] : 0);
+        if (i < nb) bsum[i] = excl;
+        __syncthreads();
+        if (threadIdx.x == kScanThreads - 1) carry = excl + t;
+        __syncthreads();
+    }
+}
+// pass 3: add the scanned block totals
+__global__ void k_scan_add(int *__restrict__ v, int n, const int *__restrict__ bsum) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] += bsum[i / kScanBlock];
+}
+
+// particles into their slots (order within a slot still arbitrary); counts
+// run down to zero
+__global__ void k_order_fill(const int *__restrict__ slot_of, int P, const int *__restrict__ start,
+                             int *__restrict__ slot_cnt, int *__restrict__ bucket) {
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < P; g += gridDim.x * blockDim.x) {
+        const int s = slot_of[g];
+        if (s < 0) continue;
+        const int k = atomicSub(slot_cnt + s, 1) - 1;
+        bucket[start[s] + k] = g;
+    }
+}
+
+// each slot sorted by reference index (slots above `cap` particles stay
+// unsorted: the binning that follows reports them as cell overflow), then
+// the storage-order arrays
+__global__ void k_order_emit(const int *__restrict__ start, int T, int P, int cap, int *__restrict__ bucket,
+                             const float *__restrict__ pos3, const int *__restrict__ rep_of_gid,
+                             const SysDev *__restrict__ sys, float4 *__restrict__ staged, int *__restrict__ gid_of,
+                             int *__restrict__ rep_of_sid) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < T; s += gridDim.x * blockDim.x) {
+        const int a = start[s], n = (s + 1 < T ? start[s + 1] : P) - a;
+        int *bk = bucket + a;
+        if (n <= cap)
+            for (int i = 1; i < n; i++) {  // insertion sort: a cell holds a few particles
+                const int g = bk[i];
+                int j = i - 1;
+                while (j >= 0 && bk[j] > g) {
+                    bk[j + 1] = bk[j];
+                    j--;
+                }
+                bk[j + 1] = g;
+            }
+        for (int i = 0; i < n; i++) {
+            const int sid = a + i, g = bk[i];
+            const int r = rep_of_gid[g];
+            const SysDev &S = sys[r];
+            const unsigned w = (unsigned)sid | ((g - S.part_base) < S.n_big ? 0u : 1u) << 31;
+            staged[sid] = make_float4(pos3[3 * (size_t)g], pos3[3 * (size_t)g + 1], pos3[3 * (size_t)g + 2],
+                                      __uint_as_float(w));
+            gid_of[sid] = g;
+            rep_of_sid[sid] = r;
+        }
+    }
+}
+
 // ------------------------------------------------------------- load/export
 // Bin particles given in storage order (float4 w = sid | species << 31).
 __global__ void k_load(const float4 *__restrict__ staged, int P, const int *__restrict__ rep_of_sid,

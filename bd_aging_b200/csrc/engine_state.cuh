@@ -76,7 +76,15 @@ struct bd_engine {
     float4 *pbuild = nullptr;
     int *nbr = nullptr, *nnb = nullptr;
     int *lflag = nullptr, *d_one = nullptr;
-    long long *d_builds = nullptr;  // list builds so far
+    long long *d_builds = nullptr;  // [0] replica list builds, [1] steps that rebuilt
+    // set_positions scratch (storage order computed on the device)
+    float *ld_in = nullptr;        // [P][3] positions as given
+    float4 *ld_staged = nullptr;   // [P] in storage order
+    int *ld_slot = nullptr, *ld_bucket = nullptr;  // [P]
+    int *ld_cnt = nullptr, *ld_start = nullptr;    // [slots]: count, first storage id
+    int *ld_bsum = nullptr;                         // [slots / kScanBlock + 1]
+    unsigned *ld_bad = nullptr;
+    long long ld_slots = 0;        // capacity of ld_cnt
 };
 
 

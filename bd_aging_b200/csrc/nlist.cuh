@@ -11,7 +11,8 @@
 // the list was built.  The step kernel checks that for every particle and
 // raises a device flag; the rebuild kernels of the next step run only when the
 // flag is set (they exit at once otherwise), so CUDA graphs need no host
-// decision.
+// decision.  (Conditional graph nodes around the rebuild kernels, switched on
+// by the step kernel, measured 2% slower than these four early exits.)
 //
 // State by storage id: pos[2][P] float4 (double-buffered: x, y, z and
 // w = storage id | species << 31), positions at the last build, the lists
@@ -27,14 +28,14 @@ constexpr int kMaxNbr = 64;
 #ifndef BD_LIST_GATHER
 #define BD_LIST_GATHER 4  // list partners whose positions are in flight together
 #endif
-#ifndef BD_LIST_PIPE
-#define BD_LIST_PIPE 1       // load the next chunk's list words under this chunk's gathers
-#endif
 #ifndef BD_LIST_THREADS
 #define BD_LIST_THREADS 256  // CTA size of the list step
 #endif
 #ifndef BD_LIST_MINB
 #define BD_LIST_MINB 4       // resident CTAs per SM asked of the register allocator (64 registers)
+#endif
+#ifndef BD_LIST_STREAM
+#define BD_LIST_STREAM 0     // evict-first loads/stores: 1 per-particle state, 2 also list words
 #endif
 
 struct ListArgs {
@@ -67,6 +68,25 @@ struct ListArgs {
 // shortcut when |d / L| < 0.49
 __device__ __forceinline__ float min_image_fast(float d, float L, float Linv) {
     return fabsf(__fmul_rn(Linv, d)) < 0.49f ? d : min_image_f(d, L, Linv);
+}
+
+// Per-particle state is touched once per step: with BD_LIST_STREAM its loads
+// and stores take the evict-first policy, so the positions that the partner
+// gathers read stay in L2.
+template <int LEVEL, class T>
+__device__ __forceinline__ T ld_state(const T *p) {
+    if (BD_LIST_STREAM >= LEVEL) return __ldcs(p);
+    return __ldg(p);
+}
+template <class T>
+__device__ __forceinline__ T ld_state_rw(const T *p) {  // read and written by the same thread
+    if (BD_LIST_STREAM >= 1) return __ldcs(p);
+    return *p;
+}
+template <class T>
+__device__ __forceinline__ void st_state(T *p, T v) {
+    if (BD_LIST_STREAM >= 1) __stcs(p, v);
+    else *p = v;
 }
 
 // ------------------------------------------------------------- rebuild
@@ -174,9 +194,11 @@ __global__ void __launch_bounds__(192, 4) k_list_build(StepArgs a, ListBuild lb)
     }
 }
 
-// clear the flags after a rebuild; builds counts replica rebuilds
+// clear the flags after a rebuild; builds[0] counts replica rebuilds,
+// builds[1] the steps that rebuilt
 __global__ void k_list_done(int *flag, int nrep, long long *builds) {
     if (flag[nrep] == 0) return;
+    if (threadIdx.x == 0) atomicAdd((unsigned long long *)(builds + 1), 1ull);
     __syncthreads();
     for (int r = threadIdx.x; r < nrep; r += blockDim.x)
         if (flag[r]) {
@@ -188,6 +210,136 @@ __global__ void k_list_done(int *flag, int nrep, long long *builds) {
 }
 
 // ------------------------------------------------------------- step
+// Partners go in chunks of kGather: the chunk's list words (loaded one chunk
+// ahead), then all its positions in flight, then the next chunk's list words
+// under those gathers, then the pair arithmetic in list order.
+constexpr int kGather = BD_LIST_GATHER;
+static_assert(kGather % 2 == 0, "partners are paired for f32x2 arithmetic");
+
+__device__ __forceinline__ void list_words(const ListArgs &a, int sid, int n, int k0, int (&jn)[kGather]) {
+#pragma unroll
+    for (int u = 0; u < kGather; u++) {
+        const int k = k0 + u;
+        jn[u] = (k < n) ? ld_state<2>(a.nbr + (size_t)k * a.np + sid) : -1;
+    }
+}
+// positions of the chunk's partners; an absent or out-of-range entry reads
+// as index -1 at the origin
+__device__ __forceinline__ void gather_chunk(const ListArgs &a, const int (&jn)[kGather], int (&jj)[kGather],
+                                             float4 (&pj)[kGather]) {
+#pragma unroll
+    for (int u = 0; u < kGather; u++) {
+        jj[u] = jn[u];
+        const bool ok = (unsigned)jj[u] < (unsigned)a.np;
+        if (jj[u] >= 0 && !ok) set_status(a.status, kStatArg);  // never true for consistent lists
+        pj[u] = ok ? __ldg(a.pos_in + jj[u]) : make_float4(0.f, 0.f, 0.f, 0.f);
+        if (!ok) jj[u] = -1;
+    }
+}
+
+// Modified-WCA force on one particle from its list, two partners per f32x2
+// operation (each lane rounds as the scalar operation does).  WRAP: a
+// partner may lie across the periodic boundary, so each displacement takes
+// the reference minimum image; otherwise every partner is within the box
+// around the particle and the minimum image would return the plain
+// difference.  The force is summed in two interleaved partial sums (even and
+// odd list positions) that are added at the end.
+template <bool WRAP>
+__device__ __forceinline__ void list_forces_wca(const ListArgs &a, int sid, int n, float4 pi, float L, float Linv,
+                                                float sg0, float sg1, float c0, float c1, float &fx, float &fy,
+                                                float &fz) {
+    const f2 PX = f2_bcast(pi.x), PY = f2_bcast(pi.y), PZ = f2_bcast(pi.z), M12 = f2_bcast(-12.0f);
+    f2 FX = 0ull, FY = 0ull, FZ = 0ull;  // (0.f, 0.f)
+    int jn[kGather];
+    list_words(a, sid, n, 0, jn);
+    for (int k0 = 0; k0 < n; k0 += kGather) {
+        int jj[kGather];
+        float4 pj[kGather];
+        gather_chunk(a, jn, jj, pj);
+        list_words(a, sid, n, k0 + kGather, jn);
+#pragma unroll
+        for (int u = 0; u < kGather; u += 2) {
+            const float4 qa = pj[u], qb = pj[u + 1];
+            f2 dX = f2_sub(f2_make(qa.x, qb.x), PX);
+            f2 dY = f2_sub(f2_make(qa.y, qb.y), PY);
+            f2 dZ = f2_sub(f2_make(qa.z, qb.z), PZ);
+            if (WRAP) {
+                float xa, xb, ya, yb, za, zb;
+                f2_split(dX, xa, xb);
+                f2_split(dY, ya, yb);
+                f2_split(dZ, za, zb);
+                dX = f2_make(min_image_fast(xa, L, Linv), min_image_fast(xb, L, Linv));
+                dY = f2_make(min_image_fast(ya, L, Linv), min_image_fast(yb, L, Linv));
+                dZ = f2_make(min_image_fast(za, L, Linv), min_image_fast(zb, L, Linv));
+            }
+            // dist2_rn in each lane
+            const f2 D2 = f2_add(f2_add(f2_mul(dX, dX), f2_mul(dY, dY)), f2_mul(dZ, dZ));
+            float d2a, d2b;
+            f2_split(D2, d2a, d2b);
+            const bool ta = (__float_as_uint(qa.w) >> 31) != 0u, tb = (__float_as_uint(qb.w) >> 31) != 0u;
+            const bool oka = jj[u] >= 0 && d2a < (ta ? c1 : c0);
+            const bool okb = jj[u + 1] >= 0 && d2b < (tb ? c1 : c0);
+            if (oka || okb) {
+                const f2 DI = f2_make(rsqrtf(d2a), rsqrtf(d2b));
+                const f2 SOR = f2_mul(DI, f2_make(ta ? sg1 : sg0, tb ? sg1 : sg0));
+                const f2 S2 = f2_mul(SOR, SOR);
+                const f2 S6 = f2_mul(f2_mul(S2, S2), S2);
+                // -12 (s^12 - s^6) / r^2
+                const f2 G = f2_mul(f2_mul(M12, f2_sub(f2_mul(S6, S6), S6)), f2_mul(DI, DI));
+                float ga, gb;
+                f2_split(G, ga, gb);
+                const f2 GM = f2_make(oka ? ga : 0.f, okb ? gb : 0.f);
+                FX = f2_fma(GM, dX, FX);
+                FY = f2_fma(GM, dY, FY);
+                FZ = f2_fma(GM, dZ, FZ);
+            }
+        }
+    }
+    float ea, eb;
+    f2_split(FX, ea, eb);
+    fx = __fadd_rn(ea, eb);
+    f2_split(FY, ea, eb);
+    fy = __fadd_rn(ea, eb);
+    f2_split(FZ, ea, eb);
+    fz = __fadd_rn(ea, eb);
+}
+
+// Force from the list for a replica with another potential of PotKind
+// (scalar, list order).
+__device__ __forceinline__ void list_forces_extra(const ListArgs &a, const SysDev &S, int sid, int n, float4 pi, int tm,
+                                               float &fx, float &fy, float &fz) {
+    const float L = S.L, Linv = S.Linv;
+    const float sg0 = tm ? S.sig[1] : S.sig[0], sg1 = tm ? S.sig[2] : S.sig[1];
+    const float c0 = tm ? S.cut2[1] : S.cut2[0], c1 = tm ? S.cut2[2] : S.cut2[1];
+    fx = fy = fz = 0.f;
+    int jn[kGather];
+    list_words(a, sid, n, 0, jn);
+    for (int k0 = 0; k0 < n; k0 += kGather) {
+        int jj[kGather];
+        float4 pj[kGather];
+        gather_chunk(a, jn, jj, pj);
+        list_words(a, sid, n, k0 + kGather, jn);
+#pragma unroll
+        for (int u = 0; u < kGather; u++) {
+            if (jj[u] < 0) continue;
+            const float dx = min_image_fast(__fsub_rn(pj[u].x, pi.x), L, Linv);
+            const float dy = min_image_fast(__fsub_rn(pj[u].y, pi.y), L, Linv);
+            const float dz = min_image_fast(__fsub_rn(pj[u].z, pi.z), L, Linv);
+            const float d2 = dist2_rn(dx, dy, dz);
+            const bool tj = (__float_as_uint(pj[u].w) >> 31) != 0u;
+            if (d2 < (tj ? c1 : c0)) {
+                const float sg = tj ? sg1 : sg0;
+                const float di = rsqrtf(d2);
+                float uu = 0.f;
+                const float g = pair_extra(S.pot, S.pp, sg, di, &uu);
+                fx = fmaf(g, dx, fx);
+                fy = fmaf(g, dy, fy);
+                fz = fmaf(g, dz, fz);
+            }
+        }
+    }
+}
+
 // One time step of every particle from its list (thread per storage id).
 // Force sum in list order; update, compensated position and FP64
 // displacement exactly as process_brick.
@@ -207,71 +359,24 @@ __global__ void __launch_bounds__(BD_LIST_THREADS, BD_LIST_MINB) k_step_list(Lis
     const float sg0 = tm ? S.sig[1] : S.sig[0], sg1 = tm ? S.sig[2] : S.sig[1];
     const float c0 = tm ? S.cut2[1] : S.cut2[0], c1 = tm ? S.cut2[2] : S.cut2[1];
     // own state early: its latency overlaps the force loop
-    const int gid = __ldg(a.gid_of + sid);
-    float lx = a.lo_x[sid], ly = a.lo_y[sid], lz = a.lo_z[sid];
-    double qx = a.dsp_x[sid], qy = a.dsp_y[sid], qz = a.dsp_z[sid];
-    const float4 pb = __ldg(a.pbuild + sid);
-    float fx = 0.f, fy = 0.f, fz = 0.f;
-    const int n = min(a.nnb[sid], kMaxNbr);
-    // partners in chunks of kGather: all list words, then all positions in
-    // flight, then the pair arithmetic in list order
-    constexpr int kGather = BD_LIST_GATHER;
-    // the list words of the next chunk load while this chunk's positions do
-    int jn[kGather];
-#pragma unroll
-    for (int u = 0; u < kGather; u++) jn[u] = (u < n) ? __ldg(a.nbr + (size_t)u * a.np + sid) : -1;
-    for (int k0 = 0; k0 < n; k0 += kGather) {
-        int jj[kGather];
-        float4 pj[kGather];
-#pragma unroll
-        for (int u = 0; u < kGather; u++) {
-            jj[u] = jn[u];
-            const bool ok = (unsigned)jj[u] < (unsigned)a.np;
-            if (jj[u] >= 0 && !ok) set_status(a.status, kStatArg);  // never true for consistent lists
-            pj[u] = ok ? __ldg(a.pos_in + jj[u]) : make_float4(0.f, 0.f, 0.f, 0.f);
-            if (!ok) jj[u] = -1;
-        }
-#if BD_LIST_PIPE
-#pragma unroll
-        for (int u = 0; u < kGather; u++) {
-            const int k = k0 + kGather + u;
-            jn[u] = (k < n) ? __ldg(a.nbr + (size_t)k * a.np + sid) : -1;
-        }
-#endif
-#pragma unroll
-        for (int u = 0; u < kGather; u++) {
-            if (jj[u] < 0) continue;
-            const float dx = min_image_fast(__fsub_rn(pj[u].x, pi.x), L, Linv);
-            const float dy = min_image_fast(__fsub_rn(pj[u].y, pi.y), L, Linv);
-            const float dz = min_image_fast(__fsub_rn(pj[u].z, pi.z), L, Linv);
-            const float d2 = dist2_rn(dx, dy, dz);
-            const bool tj = (__float_as_uint(pj[u].w) >> 31) != 0u;
-            if (d2 < (tj ? c1 : c0)) {
-                const float sg = tj ? sg1 : sg0;
-                const float di = rsqrtf(d2);
-                float g;
-                if (!EXTRA || S.pot == kPotWcaModified) {
-                    const float sor = di * sg;
-                    const float s2 = sor * sor;
-                    const float s6 = s2 * s2 * s2;
-                    const float s12 = s6 * s6;
-                    g = -12.0f * (s12 - s6) * (di * di);
-                } else {
-                    float u = 0.f;
-                    g = pair_extra(S.pot, S.pp, sg, di, &u);
-                }
-                fx = fmaf(g, dx, fx);
-                fy = fmaf(g, dy, fy);
-                fz = fmaf(g, dz, fz);
-            }
-        }
-#if !BD_LIST_PIPE
-#pragma unroll
-        for (int u = 0; u < kGather; u++) {
-            const int k = k0 + kGather + u;
-            jn[u] = (k < n) ? __ldg(a.nbr + (size_t)k * a.np + sid) : -1;
-        }
-#endif
+    const int gid = ld_state<1>(a.gid_of + sid);
+    float lx = ld_state_rw(a.lo_x + sid), ly = ld_state_rw(a.lo_y + sid), lz = ld_state_rw(a.lo_z + sid);
+    double qx = ld_state_rw(a.dsp_x + sid), qy = ld_state_rw(a.dsp_y + sid), qz = ld_state_rw(a.dsp_z + sid);
+    const float4 pb = ld_state<1>(a.pbuild + sid);
+    float fx, fy, fz;
+    const int n = min(ld_state<1>(a.nnb + sid), kMaxNbr);
+    if (EXTRA && S.pot != kPotWcaModified) {
+        list_forces_extra(a, S, sid, n, pi, tm, fx, fy, fz);
+    } else {  // the same arithmetic in either instantiation: a replica's result does not depend on its batch
+        // a warp whose particles all sit away from the faces needs no
+        // minimum image for any partner
+        const float lo_edge = S.interior, hi_edge = L - S.interior;
+        const bool inner = pi.x >= lo_edge && pi.x <= hi_edge && pi.y >= lo_edge && pi.y <= hi_edge &&
+                           pi.z >= lo_edge && pi.z <= hi_edge;
+        if (__all_sync(__activemask(), inner))
+            list_forces_wca<false>(a, sid, n, pi, L, Linv, sg0, sg1, c0, c1, fx, fy, fz);
+        else
+            list_forces_wca<true>(a, sid, n, pi, L, Linv, sg0, sg1, c0, c1, fx, fy, fz);
     }
     if (S.fcap > 0.f) {  // capped forces for the initial relaxation
         const float fmx = fmaxf(fabsf(fx), fmaxf(fabsf(fy), fabsf(fz)));
@@ -320,12 +425,12 @@ __global__ void __launch_bounds__(BD_LIST_THREADS, BD_LIST_MINB) k_step_list(Lis
     qx += (double)ex;
     qy += (double)ey;
     qz += (double)ez;
-    a.lo_x[sid] = lx;
-    a.lo_y[sid] = ly;
-    a.lo_z[sid] = lz;
-    a.dsp_x[sid] = qx;
-    a.dsp_y[sid] = qy;
-    a.dsp_z[sid] = qz;
+    st_state(a.lo_x + sid, lx);
+    st_state(a.lo_y + sid, ly);
+    st_state(a.lo_z + sid, lz);
+    st_state(a.dsp_x + sid, qx);
+    st_state(a.dsp_y + sid, qy);
+    st_state(a.dsp_z + sid, qz);
     if (!(isfinite(x) && isfinite(y) && isfinite(z))) set_status(a.status, kStatNumeric);
     a.pos_out[sid] = make_float4(x, y, z, pi.w);
     // skin check against the positions at the last build

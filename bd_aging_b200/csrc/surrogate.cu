@@ -47,16 +47,16 @@ EncodeTiledFn encode_fn() {
     return fn;
 }
 
-// 2-D BF16 row-major matrix [rows][cols] as a TMA map with a 64 x 128 box
-// (64 columns = 128 bytes, 128-byte swizzle); out-of-range rows and
-// columns read as zero.
-int make_tmap(CUtensorMap *map, const void *ptr, int rows, int cols) {
+// 2-D BF16 row-major matrix [rows][cols] as a TMA map with a box of 64
+// columns (128 bytes, 128-byte swizzle) by box_rows rows (kBM for A
+// operands, kBN for B operands); out-of-range rows and columns read as zero.
+int make_tmap(CUtensorMap *map, const void *ptr, int rows, int cols, int box_rows) {
     EncodeTiledFn enc = encode_fn();
     if (!enc) return BD_ERR_CUDA;
     if ((reinterpret_cast<uintptr_t>(ptr) & 15) || (cols % 8)) return BD_ERR_ARG;
     cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
-    cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)kBM};
+    cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(ptr), dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -430,7 +430,7 @@ int bd_surrogate_create(int n_in, int n_out, int width, int depth, int batch, un
     A((void **)&s->t, (size_t)batch * 128 * 4);
     A((void **)&s->tw, 128 * 4);
     A((void **)&s->part, part_total * 4);
-    s->loss_cells = (batch / kBM) * 1;
+    s->loss_cells = (batch / kBM) * div_up(s->Np[s->L - 1], kBN);  // CTAs of the output GEMM
     A((void **)&s->loss_part, (size_t)s->loss_cells * 4);
     A((void **)&s->step, sizeof(long long));
     A((void **)&s->err, sizeof(unsigned));
@@ -464,12 +464,14 @@ int bd_surrogate_create(int n_in, int n_out, int width, int depth, int batch, un
     s->tm_wb.resize(s->L);
     s->tm_wbt.resize(s->L);
     for (int l = 0; l < s->L && !rc; l++) {
-        rc |= make_tmap(&s->tm_h[l], s->h[l], batch, s->Kp[l]);
-        rc |= make_tmap(&s->tm_ht[l], s->ht[l], s->Kp[l], batch);
-        rc |= make_tmap(&s->tm_dz[l], s->dz[l], batch, s->Np[l]);
-        rc |= make_tmap(&s->tm_dzt[l], s->dzt[l], s->Np[l], batch);
-        rc |= make_tmap(&s->tm_wb[l], s->wb[l], s->Np[l], s->Kp[l]);
-        rc |= make_tmap(&s->tm_wbt[l], s->wbt[l], s->Kp[l], s->Np[l]);
+        // A operands: h (forward), dz^T (weight gradient), dz (input gradient);
+        // B operands: W, h^T, W^T
+        rc |= make_tmap(&s->tm_h[l], s->h[l], batch, s->Kp[l], kBM);
+        rc |= make_tmap(&s->tm_ht[l], s->ht[l], s->Kp[l], batch, kBN);
+        rc |= make_tmap(&s->tm_dz[l], s->dz[l], batch, s->Np[l], kBM);
+        rc |= make_tmap(&s->tm_dzt[l], s->dzt[l], s->Np[l], batch, kBM);
+        rc |= make_tmap(&s->tm_wb[l], s->wb[l], s->Np[l], s->Kp[l], kBN);
+        rc |= make_tmap(&s->tm_wbt[l], s->wbt[l], s->Kp[l], s->Np[l], kBN);
     }
     if (rc || cudaStreamSynchronize(s->stream) != cudaSuccess) {
         free_surrogate(s);
@@ -694,8 +696,8 @@ int bd_umma_gemm_bf16(const unsigned short *a, const unsigned short *b, int M, i
         cudaMemcpyAsync(da, a, (size_t)M * K * 2, cudaMemcpyHostToDevice, st);
         cudaMemcpyAsync(db, b, (size_t)N * K * 2, cudaMemcpyHostToDevice, st);
         cudaMemsetAsync(err, 0, 4, st);
-        rc = make_tmap(&ta, da, M, K);
-        if (!rc) rc = make_tmap(&tb, db, N, K);
+        rc = make_tmap(&ta, da, M, K, kBM);
+        if (!rc) rc = make_tmap(&tb, db, N, K, kBN);
     }
     if (!rc) {
         GemmArgs g;

@@ -2,13 +2,15 @@
 // surrogate network: C[M][N] = sum_k A[M][k] B[N][k] (both operands
 // K-major, BF16; FP32 accumulation in tensor memory) with fused epilogues.
 //
-// One CTA (8 warps) computes a 128 x 128 tile over a K range of at most 256:
+// One CTA (8 warps) computes a 128 x 64 tile over a K range of at most 256:
 //   * thread 0 issues every TMA load of the range at once (64-wide K chunks,
 //     128-byte swizzle, one mbarrier per chunk, no multicast);
-//   * one lane of warp 1 issues tcgen05.mma (M=128, N=128, K=16) per 16-wide
+//   * one lane of warp 1 issues tcgen05.mma (M=128, N=64, K=16) per 16-wide
 //     slice as each chunk lands, then tcgen05.commit to the "done" barrier;
 //   * all eight warps read accumulator rows with tcgen05.ld (warp w: lanes
 //     32 (w % 4) .. + 31, the column half w / 4) and apply the epilogue.
+// The 64-wide N tile gives the small surrogate GEMMs (N = 256) four column
+// tiles, so 128 CTAs share the epilogue work instead of 64.
 // Every mbarrier wait is bounded: on expiry the CTA records an error flag,
 // waits (bounded) for its own copies, frees its tensor memory and returns.
 #pragma once
@@ -21,11 +23,13 @@
 namespace bd {
 namespace umma {
 
-constexpr int kBM = 128, kBN = 128, kBK = 64;  // kBK bf16 = one 128-byte swizzle row
-constexpr int kMaxChunks = 4;                   // K range per CTA <= 256
-constexpr int kThreads = 256;  // 8 warps: warp w reads TMEM lanes 32 (w % 4), columns 64 (w / 4)
-constexpr int kStageBytes = kBM * kBK * 2;      // 16 KB per operand tile
-constexpr int kSmemBytes = 2 * kMaxChunks * kStageBytes + 1024 /* align */ + 256 /* barriers */;
+constexpr int kBM = 128, kBN = 64, kBK = 64;  // kBK bf16 = one 128-byte swizzle row
+constexpr int kMaxChunks = 4;                  // K range per CTA <= 256
+constexpr int kThreads = 256;  // 8 warps: warp w reads TMEM lanes 32 (w % 4), columns kBN / 2 (w / 4)
+constexpr int kStageA = kBM * kBK * 2;         // 16 KB per A tile
+constexpr int kStageB = kBN * kBK * 2;         // 8 KB per B tile
+constexpr int kSmemBytes = kMaxChunks * (kStageA + kStageB) + 1024 /* align */ + 256 /* barriers */;
+static_assert(kBN % 64 == 0, "two column halves of whole 32-column groups");
 constexpr long kSpinLimit = 1L << 20;
 
 enum Epilogue {
@@ -148,9 +152,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     extern __shared__ unsigned char smem_raw[];
     unsigned char *smem =
         reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    unsigned char *sA = smem;                              // [kMaxChunks][16 KB]
-    unsigned char *sB = smem + kMaxChunks * kStageBytes;   // [kMaxChunks][16 KB]
-    uint64_t *full = reinterpret_cast<uint64_t *>(smem + 2 * kMaxChunks * kStageBytes);
+    unsigned char *sA = smem;                          // [kMaxChunks][kStageA]
+    unsigned char *sB = smem + kMaxChunks * kStageA;   // [kMaxChunks][kStageB]
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + kMaxChunks * (kStageA + kStageB));
     uint64_t *done = full + kMaxChunks;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
     __shared__ float red[kThreads / 32];
@@ -179,9 +183,9 @@ __global__ void __launch_bounds__(kThreads, 1)
 
     if (threadIdx.x == 0) {
         for (int c = 0; c < nk; c++) {
-            mbar_expect_tx(&full[c], 2 * kStageBytes);
-            tma_load_2d(sA + c * kStageBytes, &tmA, &full[c], kb + c * kBK, m0);
-            tma_load_2d(sB + c * kStageBytes, &tmB, &full[c], kb + c * kBK, n0);
+            mbar_expect_tx(&full[c], kStageA + kStageB);
+            tma_load_2d(sA + c * kStageA, &tmA, &full[c], kb + c * kBK, m0);
+            tma_load_2d(sB + c * kStageB, &tmB, &full[c], kb + c * kBK, n0);
         }
     }
     if (warp == 1 && lane == 0) {
@@ -190,8 +194,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             ok = mbar_wait(&full[c], 0, g.err, 1u);
             if (!ok) break;
             tc_fence_after();
-            const uint64_t ad = smem_desc_sw128(smem_u32(sA + c * kStageBytes));
-            const uint64_t bd = smem_desc_sw128(smem_u32(sB + c * kStageBytes));
+            const uint64_t ad = smem_desc_sw128(smem_u32(sA + c * kStageA));
+            const uint64_t bd = smem_desc_sw128(smem_u32(sB + c * kStageB));
 #pragma unroll
             for (int kk = 0; kk < kBK / 16; kk++)  // 16 bf16 = 32 bytes = 2 descriptor units
                 umma_bf16(tmem, ad + 2 * kk, bd + 2 * kk, (c | kk) ? 1u : 0u);

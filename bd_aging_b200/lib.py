@@ -86,7 +86,7 @@ class EngineInfo(C.Structure):
                 ("brick", C.c_int * 3), ("threads", C.c_int), ("cell_capacity", C.c_int),
                 ("staging_capacity", C.c_int), ("mode", C.c_int), ("cluster", C.c_int),
                 ("smem_bytes", C.c_size_t), ("next_step", C.c_longlong), ("neighbor_skin", C.c_float),
-                ("list_builds", C.c_longlong)]
+                ("list_builds", C.c_longlong), ("list_rebuild_steps", C.c_longlong)]
 
 
 _LIB = None
@@ -422,9 +422,16 @@ class Engine:
         _check(_lib().bd_engine_observe(self._h, out), "observe")
         return [o.as_dict() for o in out]
 
-    def get_positions(self):
-        pos = np.zeros((self.P, 3), np.float32)
-        raw = np.zeros((self.P, 3), np.float32)
+    def get_positions(self, out_pos: np.ndarray = None, out_raw: np.ndarray = None):
+        """Wrapped and unwrapped positions [P, 3] by reference index, written
+        into out_pos / out_raw when given (C-contiguous float32, e.g. pinned)."""
+        def buf(a):
+            if a is None:
+                return np.empty((self.P, 3), np.float32)
+            if a.dtype != np.float32 or a.shape != (self.P, 3) or not a.flags.c_contiguous:
+                raise ValueError("output buffers must be C-contiguous float32 [P, 3]")
+            return a
+        pos, raw = buf(out_pos), buf(out_raw)
         _check(_lib().bd_engine_get_positions(self._h, _ptr(pos), _ptr(raw)), "get_positions")
         return pos, raw
 

@@ -454,6 +454,7 @@ def run_ours(args):
     ms = ranks.max_over_ranks(ms)
     ranks.barrier()
     ck = clocks.stop()
+    rebuild_steps = eng.info().list_rebuild_steps - info.list_rebuild_steps
     total_ps = P * S * args.steps * world
     value = total_ps / (ms / 1e3)
     launches = S * args.steps
@@ -463,8 +464,10 @@ def run_ours(args):
     list_mode = info.neighbor_skin > 0
     tpp = profile_traffic_per_particle_step(list_mode)
     # kernels per time step: the list step plus its four rebuild kernels (which
-    # exit at once when no list is stale), or the one sweep kernel
+    # exit at once when no list is stale), or the one sweep kernel; per
+    # 96-step graph the counter kernel (persistent mode: one launch per graph)
     per_step = 5 if list_mode else (1 if args.mode == "plain" else 0)
+    gpu_launches = args.steps * (math.ceil(S / 96) * (1 if per_step else 2) + per_step * S)
     line = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 forces, f32+compensation positions, f64 displacement",
@@ -474,8 +477,9 @@ def run_ours(args):
                            brick=list(info.brick), threads=info.threads, cell_capacity=info.cell_capacity,
                            mode=args.mode, cluster=info.cluster if args.mode == "persistent" else None,
                            neighbor_skin=info.neighbor_skin, list_builds=info.list_builds,
+                           list_rebuild_steps_timed=int(rebuild_steps),
                            autotune=bool(args.autotune)),
-            "gpu_launches": int(args.steps * (math.ceil(S / 96) * (1 if per_step else 2) + per_step * S)),
+            "gpu_launches": int(gpu_launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "alg_bytes_per_launch": ALG_BYTES_PER_PARTICLE_STEP * P,
@@ -498,18 +502,22 @@ def run_ours(args):
         e1.close()
         line["plain"] = {"value": plain, "unit": "particle-steps/s", "replicas": 1}
         line["batched_over_plain"] = value / plain
-        # end to end through the C ABI with host buffers
-        out_pos = np.zeros((P, 3), np.float32)
+        # end to end through the C ABI with pinned host buffers: positions in,
+        # wrapped and unwrapped positions out, every step
+        def pinned():
+            return torch.empty((P, 3), dtype=torch.float32, pin_memory=True).numpy()
+        in_pos, out_pos, out_raw = pinned(), pinned(), pinned()
+        in_pos[:] = pos
 
         def e2e_step():
-            eng.set_positions(pos)
+            eng.set_positions(in_pos)
             eng.run(S)
-            out_pos[:] = eng.get_positions()[0]
+            eng.get_positions(out_pos, out_raw)
         e2e_step()
         ms2 = cuda_time(eng, e2e_step, max(2, args.steps // 2))
         k2 = max(2, args.steps // 2)
         line["e2e"] = {"value": P * S * k2 / (ms2 / 1e3), "unit": "particle-steps/s",
-                       "h2d_bytes_per_step": P * (16 + 4 + 4), "d2h_bytes_per_step": P * 24}
+                       "h2d_bytes_per_step": P * 12, "d2h_bytes_per_step": P * 24}
         try:
             line["reference_cuda"] = reference_cuda()
             if line["reference_cuda"] and "value" in line["reference_cuda"]:

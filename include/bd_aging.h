@@ -294,7 +294,8 @@ typedef struct bd_engine_info {
     size_t smem_bytes;
     long long next_step;          /* reference ni of the next update */
     float neighbor_skin;          /* 0 when the engine sweeps every step */
-    long long list_builds;        /* neighbour-list builds so far */
+    long long list_builds;        /* neighbour-list builds so far (per replica) */
+    long long list_rebuild_steps; /* time steps that rebuilt some replica's lists */
 } bd_engine_info;
 
 void bd_engine_opts_default(bd_engine_opts *opts);

@@ -127,6 +127,23 @@ def test_cell_capacity_overflow_raises():
     assert ei.value.code == 3
 
 
+def test_set_positions_rejects_positions_outside_the_box():
+    # the storage order is computed on the device; a position outside [0, L]
+    # or NaN is an argument error that leaves the loaded state as it was
+    s, pos = system(500, 500, 0.5, 8)
+    e = B.Engine([s])
+    e.set_positions(pos)
+    before = e.get_positions()[0]
+    for bad in (np.nan, -1e-3, s.side * 1.001):
+        p2 = pos.copy()
+        p2[777, 1] = bad
+        with pytest.raises(B.BDError) as ei:
+            e.set_positions(p2)
+        assert ei.value.code == B.BD_ERR_ARG
+    np.testing.assert_array_equal(e.get_positions()[0], before)
+    e.run(10)  # still usable
+
+
 def test_nan_temperature_of_instant_quench_is_reported():
     # t0 == tf == 0 (run-fself.sh:30-31) gives T = NaN at t == 0 in the
     # reference (set_temp.cu:10-11); the next update turns positions into NaN.

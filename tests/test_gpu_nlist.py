@@ -94,6 +94,32 @@ def test_list_batched_equals_plain_and_graph_equals_single_steps():
     for _ in range(250):
         e2.run(1)
     np.testing.assert_array_equal(e2.get_positions()[0], pb)
+    # rebuilds inside graphs (conditional nodes) happen at the same steps as
+    # in single-step launches
+    ib, i2 = eb.info(), e2.info()
+    assert ib.list_rebuild_steps == i2.list_rebuild_steps > 3
+    assert ib.list_builds == i2.list_builds
+
+
+def test_list_graph_rebuilds_only_when_flagged():
+    # a cold system whose particles stay within half the skin: one build, and
+    # graph runs launch no rebuild bodies; a hot one rebuilds inside graphs
+    s, pos = system(800, 800, 0.5, 12, T0=1e-4, protocol="const", dt=1e-6)
+    e = B.Engine([s], neighbor_skin=SKIN, graph_steps=96)
+    e.set_positions(pos)
+    e.run(96 * 3)
+    assert e.info().list_rebuild_steps == 1 and e.info().list_builds == 1
+    s, pos = system(800, 800, 0.5, 12, T0=2.0, protocol="const", dt=2e-4)
+    e = B.Engine([s], neighbor_skin=SKIN, graph_steps=96)
+    e.set_positions(pos)
+    e.run(96 * 3)
+    hot = e.info().list_rebuild_steps
+    assert hot > 6
+    hi, _ = e.get_positions()
+    cnt, hsh = e.census()
+    _, _, _, nbr, h = O.eng_forces(hi, types_of(s), s.side, SB, SS)
+    np.testing.assert_array_equal(cnt, nbr)
+    np.testing.assert_array_equal(hsh, h)
 
 
 def test_list_observables_match_oracle():
