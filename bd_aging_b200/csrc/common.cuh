@@ -29,6 +29,7 @@ __device__ __forceinline__ void set_status(unsigned *st, unsigned bits) {
     if (st) atomicOr(st, bits);
 }
 
+
 // ------------------------------------------------------------ minimum image
 // get_forces.cu:389-391: d -= side * floor(side_inv * d + 0.5f)  (float)
 __device__ __forceinline__ float min_image_f(float d, float side, float side_inv) {

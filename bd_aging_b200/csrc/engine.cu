@@ -620,8 +620,12 @@ int bd_engine_create(const bd_system_desc *systems, int nsys, const bd_engine_op
         ALLOC(e->rn_lcg, sizeof(unsigned long long) * P);
     }
     if (e->list) {
-        ALLOC(e->lpos[0], sizeof(float4) * P);
-        ALLOC(e->lpos[1], sizeof(float4) * P);
+        // one more entry: storage id P is the zero position that padded list
+        // entries gather (never written after this)
+        ALLOC(e->lpos[0], sizeof(float4) * (P + 1));
+        ALLOC(e->lpos[1], sizeof(float4) * (P + 1));
+        cudaMemsetAsync(e->lpos[0], 0, sizeof(float4) * (P + 1), e->stream);
+        cudaMemsetAsync(e->lpos[1], 0, sizeof(float4) * (P + 1), e->stream);
         ALLOC(e->pbuild, sizeof(float4) * P);
         ALLOC(e->nbr, sizeof(int) * (size_t)kMaxNbr * P);
         ALLOC(e->nnb, sizeof(int) * P);

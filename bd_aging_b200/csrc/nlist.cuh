@@ -37,6 +37,8 @@ constexpr int kMaxNbr = 64;
 #ifndef BD_LIST_STREAM
 #define BD_LIST_STREAM 0     // evict-first loads/stores: 1 per-particle state, 2 also list words
 #endif
+constexpr int kGather = BD_LIST_GATHER;
+static_assert(kGather % 2 == 0 && kMaxNbr % kGather == 0, "partners are paired for f32x2 arithmetic");
 
 struct ListArgs {
     const SysDev *sys;
@@ -183,7 +185,10 @@ __global__ void __launch_bounds__(192, 4) k_list_build(StepArgs a, ListBuild lb)
                     }
                 flush();
                 if (ok_sid) {
-                    lb.nnb[home_sid] = min(cnt, kMaxNbr);
+                    const int nl = min(cnt, kMaxNbr);
+                    // pad to whole gather chunks with storage id np (the zero position)
+                    for (int k = nl; k < kMaxNbr && (k % kGather) != 0; k++) lb.nbr[(size_t)k * a.np + home_sid] = a.np;
+                    lb.nnb[home_sid] = nl;
                     lb.pbuild[home_sid] = lb.pos_sid[home_sid];
                 } else {
                     set_status(a.status, kStatArg);
@@ -212,28 +217,23 @@ __global__ void k_list_done(int *flag, int nrep, long long *builds) {
 // ------------------------------------------------------------- step
 // Partners go in chunks of kGather: the chunk's list words (loaded one chunk
 // ahead), then all its positions in flight, then the next chunk's list words
-// under those gathers, then the pair arithmetic in list order.
-constexpr int kGather = BD_LIST_GATHER;
-static_assert(kGather % 2 == 0, "partners are paired for f32x2 arithmetic");
+// under those gathers, then the pair arithmetic in list order.  Lists are
+// padded to whole chunks with storage id np, whose position entry is zero and
+// never written, so a chunk needs no per-entry length test.
 
-__device__ __forceinline__ void list_words(const ListArgs &a, int sid, int n, int k0, int (&jn)[kGather]) {
+// list words k0 .. k0 + kGather - 1 (k0 < kMaxNbr)
+__device__ __forceinline__ void list_words(const ListArgs &a, int sid, int k0, int (&jn)[kGather]) {
 #pragma unroll
-    for (int u = 0; u < kGather; u++) {
-        const int k = k0 + u;
-        jn[u] = (k < n) ? ld_state<2>(a.nbr + (size_t)k * a.np + sid) : -1;
-    }
+    for (int u = 0; u < kGather; u++) jn[u] = ld_state<2>(a.nbr + (size_t)(k0 + u) * a.np + sid);
 }
-// positions of the chunk's partners; an absent or out-of-range entry reads
-// as index -1 at the origin
+// positions of the chunk's partners: an entry outside [0, np) reads the zero
+// position at np and counts as absent (jj = np)
 __device__ __forceinline__ void gather_chunk(const ListArgs &a, const int (&jn)[kGather], int (&jj)[kGather],
                                              float4 (&pj)[kGather]) {
 #pragma unroll
     for (int u = 0; u < kGather; u++) {
-        jj[u] = jn[u];
-        const bool ok = (unsigned)jj[u] < (unsigned)a.np;
-        if (jj[u] >= 0 && !ok) set_status(a.status, kStatArg);  // never true for consistent lists
-        pj[u] = ok ? __ldg(a.pos_in + jj[u]) : make_float4(0.f, 0.f, 0.f, 0.f);
-        if (!ok) jj[u] = -1;
+        jj[u] = (int)min((unsigned)jn[u], (unsigned)a.np);
+        pj[u] = __ldg(a.pos_in + jj[u]);
     }
 }
 
@@ -250,13 +250,14 @@ __device__ __forceinline__ void list_forces_wca(const ListArgs &a, int sid, int 
                                                 float &fz) {
     const f2 PX = f2_bcast(pi.x), PY = f2_bcast(pi.y), PZ = f2_bcast(pi.z), M12 = f2_bcast(-12.0f);
     f2 FX = 0ull, FY = 0ull, FZ = 0ull;  // (0.f, 0.f)
+    const int np = a.np;
     int jn[kGather];
-    list_words(a, sid, n, 0, jn);
+    if (n > 0) list_words(a, sid, 0, jn);
     for (int k0 = 0; k0 < n; k0 += kGather) {
         int jj[kGather];
         float4 pj[kGather];
         gather_chunk(a, jn, jj, pj);
-        list_words(a, sid, n, k0 + kGather, jn);
+        if (k0 + kGather < n) list_words(a, sid, k0 + kGather, jn);
 #pragma unroll
         for (int u = 0; u < kGather; u += 2) {
             const float4 qa = pj[u], qb = pj[u + 1];
@@ -277,8 +278,10 @@ __device__ __forceinline__ void list_forces_wca(const ListArgs &a, int sid, int 
             float d2a, d2b;
             f2_split(D2, d2a, d2b);
             const bool ta = (__float_as_uint(qa.w) >> 31) != 0u, tb = (__float_as_uint(qb.w) >> 31) != 0u;
-            const bool oka = jj[u] >= 0 && d2a < (ta ? c1 : c0);
-            const bool okb = jj[u + 1] >= 0 && d2b < (tb ? c1 : c0);
+            // without WRAP the particle is farther than every cut distance from
+            // the origin, where the padding entries sit
+            const bool oka = (!WRAP || jj[u] != np) && d2a < (ta ? c1 : c0);
+            const bool okb = (!WRAP || jj[u + 1] != np) && d2b < (tb ? c1 : c0);
             if (oka || okb) {
                 const f2 DI = f2_make(rsqrtf(d2a), rsqrtf(d2b));
                 const f2 SOR = f2_mul(DI, f2_make(ta ? sg1 : sg0, tb ? sg1 : sg0));
@@ -313,15 +316,15 @@ __device__ __forceinline__ void list_forces_extra(const ListArgs &a, const SysDe
     const float c0 = tm ? S.cut2[1] : S.cut2[0], c1 = tm ? S.cut2[2] : S.cut2[1];
     fx = fy = fz = 0.f;
     int jn[kGather];
-    list_words(a, sid, n, 0, jn);
+    if (n > 0) list_words(a, sid, 0, jn);
     for (int k0 = 0; k0 < n; k0 += kGather) {
         int jj[kGather];
         float4 pj[kGather];
         gather_chunk(a, jn, jj, pj);
-        list_words(a, sid, n, k0 + kGather, jn);
+        if (k0 + kGather < n) list_words(a, sid, k0 + kGather, jn);
 #pragma unroll
         for (int u = 0; u < kGather; u++) {
-            if (jj[u] < 0) continue;
+            if (jj[u] == a.np) continue;
             const float dx = min_image_fast(__fsub_rn(pj[u].x, pi.x), L, Linv);
             const float dy = min_image_fast(__fsub_rn(pj[u].y, pi.y), L, Linv);
             const float dz = min_image_fast(__fsub_rn(pj[u].z, pi.z), L, Linv);
