@@ -223,7 +223,9 @@ __device__ __forceinline__ void two_sum(float a, float b, float &s, float &e) {
 // wraps into the periodic box by subtracting side*floor(hi/side) the same
 // exact way.  hi stays in [0, side] (side itself only through rounding, as in
 // the reference, update_ermak.cu:139-141), which cell indexing clamps.
-__device__ __forceinline__ void advance_wrap(float &hi, float &lo, float d, float side, float side_inv) {
+// Returns the number of box lengths subtracted (0 unless the particle
+// crossed a face).
+__device__ __forceinline__ float advance_wrap(float &hi, float &lo, float d, float side, float side_inv) {
     float s, e;
     two_sum(hi, d, s, e);
     float c = __fadd_rn(lo, e);
@@ -239,6 +241,7 @@ __device__ __forceinline__ void advance_wrap(float &hi, float &lo, float d, floa
     }
     hi = h2;
     lo = c;
+    return kw;
 }
 
 // Temperature protocols, set_temp.cu:7-23, same float arithmetic (the

@@ -193,6 +193,7 @@ int bd_engine_snapshot(bd_engine *e, int slot) {
         // a snapshot taken here is that origin
         BD_CUDA_TRY(cudaMemsetAsync(dst, 0, sizeof(double) * 3 * P, e->stream));
     } else {
+        if (int rc = sync_dsp(e)) return rc;
         for (int k = 0; k < 3; k++)
             BD_CUDA_TRY(cudaMemcpyAsync(dst + k * P, e->dsp[k], sizeof(double) * P, cudaMemcpyDeviceToDevice,
                                         e->stream));
@@ -218,6 +219,7 @@ int bd_engine_correlate(bd_engine *e, const int *slots, int nslots, double q, bd
     if (rc) return rc;
     if ((rc = ensure_scratch(e->corr_part, e->corr_part_cap, (size_t)e->nsegs * nslots * kCorrFields))) return rc;
     if ((rc = ensure_scratch(e->corr_out, e->corr_out_cap, (size_t)e->R * nslots * kCorrFields))) return rc;
+    if ((rc = sync_dsp(e))) return rc;
     k_corr_partial<<<e->nsegs, kCorrThreads, 0, e->stream>>>(e->d_segs, e->d_sys, e->gid_of, e->dsp[0], e->dsp[1],
                                                              e->dsp[2], e->snaps, e->P, sl, q, e->corr_part);
     BD_LAUNCH_CHECK();
@@ -251,6 +253,7 @@ int bd_engine_get_displacements(bd_engine *e, double *dsp_host) {
     const size_t n = 3 * (size_t)e->P;
     double *d = nullptr;
     BD_CUDA_TRY(cudaMalloc(&d, sizeof(double) * n));
+    if (int rc = sync_dsp(e)) return rc;
     k_export_dsp<<<div_up((long)e->P, 256), 256, 0, e->stream>>>(e->gid_of, e->dsp[0], e->dsp[1], e->dsp[2],
                                                                  (int)e->P, d);
     cudaError_t ce = cudaGetLastError();

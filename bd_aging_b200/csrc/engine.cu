@@ -235,7 +235,7 @@ ListArgs make_largs(bd_engine *e, int cur) {
     a.pos_in = e->lpos[cur & 1];
     a.pos_out = e->lpos[(cur + 1) & 1];
     a.lo_x = e->lo[0]; a.lo_y = e->lo[1]; a.lo_z = e->lo[2];
-    a.dsp_x = e->dsp[0]; a.dsp_y = e->dsp[1]; a.dsp_z = e->dsp[2];
+    a.img = e->img;
     a.nbr = e->nbr;
     a.nnb = e->nnb;
     a.pbuild = e->pbuild;
@@ -306,8 +306,27 @@ int list_step(bd_engine *e, int cur, int ni_off) {
     if (rc) return rc;
     return launch_list_step(e, make_largs(e, cur), ni_off);
 }
-// observation passes read cell buckets: rebuild them from the by-id positions
-int sync_buckets(bd_engine *e) { return e->list ? list_bin(e, e->cur, e->d_one, nullptr) : BD_OK; }
+}  // namespace
+
+// displacement of list mode rebuilt from positions, remainders and crossings
+int bd::sync_dsp(bd_engine *e) {
+    if (!e->list) return BD_OK;
+    const int c = e->cur & 1;
+    k_list_dsp<<<div_up(e->P, 256), 256, 0, e->stream>>>(e->lpos[c], e->lo[0], e->lo[1], e->lo[2], e->img, e->x0,
+                                                         e->gid_of, e->rep_of_sid, e->d_sys, (int)e->P, e->dsp[0],
+                                                         e->dsp[1], e->dsp[2]);
+    BD_LAUNCH_CHECK();
+    return BD_OK;
+}
+
+namespace {
+// observation passes read cell buckets and displacements: rebuild them from
+// the by-id state
+int sync_buckets(bd_engine *e) {
+    if (!e->list) return BD_OK;
+    int rc = sync_dsp(e);
+    return rc ? rc : list_bin(e, e->cur, e->d_one, nullptr);
+}
 
 // k steps outside graphs (k = 1 in plain mode): launch, advance the counter
 int direct_steps(bd_engine *e, int k) {
@@ -368,7 +387,7 @@ void free_engine(bd_engine *e) {
                     e->status, e->d_ni, e->out_pos, e->out_raw, e->d_cl_start, e->d_cl_bricks, e->rn_ring, e->rn_lcg,
                     e->snaps, e->d_segs, e->d_seg_first, e->corr_part, e->corr_out, e->lpos[0], e->lpos[1],
                     e->pbuild, e->nbr, e->nnb, e->lflag, e->d_one, e->d_builds, e->ld_in, e->ld_staged,
-                    e->ld_slot, e->ld_bucket, e->ld_cnt, e->ld_start, e->ld_bsum, e->ld_bad};
+                    e->ld_slot, e->ld_bucket, e->ld_cnt, e->ld_start, e->ld_bsum, e->ld_bad, e->img};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -629,6 +648,7 @@ int bd_engine_create(const bd_system_desc *systems, int nsys, const bd_engine_op
         ALLOC(e->pbuild, sizeof(float4) * P);
         ALLOC(e->nbr, sizeof(int) * (size_t)kMaxNbr * P);
         ALLOC(e->nnb, sizeof(int) * P);
+        ALLOC(e->img, sizeof(int) * 3 * P);
         ALLOC(e->lflag, sizeof(int) * (e->R + 1));
         ALLOC(e->d_one, sizeof(int));
         ALLOC(e->d_builds, 2 * sizeof(long long));
@@ -756,6 +776,7 @@ int bd_engine_set_positions(bd_engine *e, const float *pos) {
         cudaMemsetAsync(e->lo[k], 0, sizeof(float) * P, e->stream);
         cudaMemsetAsync(e->dsp[k], 0, sizeof(double) * P, e->stream);
     }
+    if (e->img) cudaMemsetAsync(e->img, 0, sizeof(int) * 3 * P, e->stream);
     cudaMemsetAsync(e->status, 0, 256, e->stream);
     e->cur = 0;
     e->generation++;  // displacement snapshots of earlier positions are void

@@ -77,6 +77,7 @@ struct bd_engine {
     int *nbr = nullptr, *nnb = nullptr;
     int *lflag = nullptr, *d_one = nullptr;
     long long *d_builds = nullptr;  // [0] replica list builds, [1] steps that rebuilt
+    int *img = nullptr;             // [3][P] face crossings since the origin (displacement on demand)
     // set_positions scratch (storage order computed on the device)
     float *ld_in = nullptr;        // [P][3] positions as given
     float4 *ld_staged = nullptr;   // [P] in storage order
@@ -100,6 +101,10 @@ int launch_gder_cells(bd_engine *e, std::vector<int> &m_of, int nbins, float ran
 // cell-bucket buffer holding the current state (list mode rebuilds buffer 0
 // before every observation pass)
 inline int obs_buf(const bd_engine *e) { return e->list ? 0 : e->cur; }
+
+// list mode keeps no per-step displacement: rebuild dsp[] from the state
+// before anything reads it (a no-op in the other modes)
+int sync_dsp(bd_engine *e);
 
 inline int engine_status(bd_engine *e) {
     unsigned bits = 0;

@@ -48,7 +48,7 @@ struct ListArgs {
     const float4 *pos_in;   // by storage id, this step
     float4 *pos_out;        // by storage id, next step
     float *lo_x, *lo_y, *lo_z;
-    double *dsp_x, *dsp_y, *dsp_z;
+    int *img;               // [3][np]: box lengths crossed per axis since the origin
     const int *nbr;         // [kMaxNbr][np]
     const int *nnb;         // [np]
     const float4 *pbuild;   // positions at the last build
@@ -364,7 +364,6 @@ __global__ void __launch_bounds__(BD_LIST_THREADS, BD_LIST_MINB) k_step_list(Lis
     // own state early: its latency overlaps the force loop
     const int gid = ld_state<1>(a.gid_of + sid);
     float lx = ld_state_rw(a.lo_x + sid), ly = ld_state_rw(a.lo_y + sid), lz = ld_state_rw(a.lo_z + sid);
-    double qx = ld_state_rw(a.dsp_x + sid), qy = ld_state_rw(a.dsp_y + sid), qz = ld_state_rw(a.dsp_z + sid);
     const float4 pb = ld_state<1>(a.pbuild + sid);
     float fx, fy, fz;
     const int n = min(ld_state<1>(a.nnb + sid), kMaxNbr);
@@ -396,10 +395,10 @@ __global__ void __launch_bounds__(BD_LIST_THREADS, BD_LIST_MINB) k_step_list(Lis
     }
     const int pid = gid - S.part_base;
     if (ni == 0) {  // origin of the unwrapped positions (main.cu:497-506)
-        qx = qy = qz = 0.0;
         a.x0[3 * (size_t)gid] = (double)pi.x + (double)lx;
         a.x0[3 * (size_t)gid + 1] = (double)pi.y + (double)ly;
         a.x0[3 * (size_t)gid + 2] = (double)pi.z + (double)lz;
+        a.img[sid] = a.img[a.np + sid] = a.img[2 * a.np + sid] = 0;
     }
     float3 xi;
     if (RNG == kRngPhilox) {
@@ -422,18 +421,18 @@ __global__ void __launch_bounds__(BD_LIST_THREADS, BD_LIST_MINB) k_step_list(Lis
     const float ey = __fadd_rn(__fmul_rn(__fmul_rn(fy, mob), dt), __fmul_rn(amp, xi.y));
     const float ez = __fadd_rn(__fmul_rn(__fmul_rn(fz, mob), dt), __fmul_rn(amp, xi.z));
     float x = pi.x, y = pi.y, z = pi.z;
-    advance_wrap(x, lx, ex, L, Linv);
-    advance_wrap(y, ly, ey, L, Linv);
-    advance_wrap(z, lz, ez, L, Linv);
-    qx += (double)ex;
-    qy += (double)ey;
-    qz += (double)ez;
+    // the displacement is not stored per step: crossings of a face are
+    // counted, and k_list_dsp rebuilds the FP64 displacement exactly from
+    // hi + lo + L * crossings - origin when an observation needs it
+    const float kx = advance_wrap(x, lx, ex, L, Linv);
+    const float ky = advance_wrap(y, ly, ey, L, Linv);
+    const float kz = advance_wrap(z, lz, ez, L, Linv);
+    if (kx != 0.f) a.img[sid] += (int)kx;
+    if (ky != 0.f) a.img[a.np + sid] += (int)ky;
+    if (kz != 0.f) a.img[2 * a.np + sid] += (int)kz;
     st_state(a.lo_x + sid, lx);
     st_state(a.lo_y + sid, ly);
     st_state(a.lo_z + sid, lz);
-    st_state(a.dsp_x + sid, qx);
-    st_state(a.dsp_y + sid, qy);
-    st_state(a.dsp_z + sid, qz);
     if (!(isfinite(x) && isfinite(y) && isfinite(z))) set_status(a.status, kStatNumeric);
     a.pos_out[sid] = make_float4(x, y, z, pi.w);
     // skin check against the positions at the last build
@@ -444,6 +443,24 @@ __global__ void __launch_bounds__(BD_LIST_THREADS, BD_LIST_MINB) k_step_list(Lis
         a.flag[a.rep_of_sid[sid]] = 1;
         a.flag[a.nrep] = 1;
     }
+}
+
+// FP64 displacement since the origin, rebuilt from the state of list mode:
+// (hi + lo) is exact in FP64 and so is L * crossings, so the only rounding is
+// the final subtraction of the origin.
+__global__ void k_list_dsp(const float4 *__restrict__ pos, const float *__restrict__ lo_x,
+                           const float *__restrict__ lo_y, const float *__restrict__ lo_z, const int *__restrict__ img,
+                           const double *__restrict__ x0, const int *__restrict__ gid_of,
+                           const int *__restrict__ rep_of_sid, const SysDev *__restrict__ sys, int np, double *dx,
+                           double *dy, double *dz) {
+    const int sid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sid >= np) return;
+    const double L = (double)sys[rep_of_sid[sid]].L;
+    const float4 v = pos[sid];
+    const size_t g = 3 * (size_t)gid_of[sid];
+    dx[sid] = (((double)v.x + (double)lo_x[sid]) + L * (double)img[sid]) - x0[g];
+    dy[sid] = (((double)v.y + (double)lo_y[sid]) + L * (double)img[np + sid]) - x0[g + 1];
+    dz[sid] = (((double)v.z + (double)lo_z[sid]) + L * (double)img[2 * (size_t)np + sid]) - x0[g + 2];
 }
 
 // Census from the lists: interacting partners per particle and a hash of
