@@ -164,3 +164,30 @@ def test_single_species_replicas_in_a_batch():
         if s.n_sml == 0:
             assert o["msd_sml"] == 0.0 and c[k]["fself_sml"] == 0.0
             assert c[k]["msd_big"] > 0.0
+
+
+def test_list_displacement_follows_face_crossings():
+    # list mode keeps no per-step displacement: face crossings are counted and
+    # the FP64 displacement is rebuilt from them.  Against the host's sum of
+    # minimum-image position increments, step by step, in a hot dilute system
+    # where many particles cross faces (and some cross back).
+    s, pos = system(300, 300, 0.2, 19, T0=6.0, protocol="const", dt=2e-4)
+    e = B.Engine([s], neighbor_skin=SKIN)
+    assert e.info().neighbor_skin > 0
+    e.set_positions(pos)
+    prev = pos.astype(np.float64)
+    acc = np.zeros_like(prev)
+    crossed = np.zeros(prev.shape, bool)
+    for _ in range(300):
+        e.run(1)
+        cur = e.get_positions()[0].astype(np.float64)
+        d = cur - prev
+        crossed |= np.abs(d) > 0.5 * s.side
+        acc += d - s.side * np.round(d / s.side)
+        prev = cur
+    got = e.get_displacements()
+    assert crossed.sum() > 50
+    np.testing.assert_allclose(got, acc, rtol=0, atol=2e-5)
+    # the unwrapped output is the origin plus the same displacement
+    _, raw = e.get_positions()
+    np.testing.assert_allclose(raw.astype(np.float64), pos.astype(np.float64) + got, rtol=0, atol=2e-5)
