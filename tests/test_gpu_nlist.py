@@ -191,3 +191,30 @@ def test_list_displacement_follows_face_crossings():
     # the unwrapped output is the origin plus the same displacement
     _, raw = e.get_positions()
     np.testing.assert_allclose(raw.astype(np.float64), pos.astype(np.float64) + got, rtol=0, atol=2e-5)
+
+
+@pytest.mark.parametrize("nb,ns,phi,seed", [(4000, 4000, 0.5, 51), (400, 400, 0.5, 52)])
+def test_list_forces_match_oracle_at_zero_temperature(nb, ns, phi, seed):
+    # T = 0: one step moves every particle by F mob dt exactly (no noise), and
+    # the FP64 displacement recovers that float increment.  Checks the list
+    # kernel's pair arithmetic (paired f32x2 lanes, padded lists, warps with
+    # and without the minimum image: the large box has interior warps, the
+    # small one nearly none) against the oracle's forces.
+    s, pos = system(nb, ns, phi, seed, T0=0.0, protocol="const", force_cap=0.0, dt=1e-6)
+    # a relaxed start keeps the forces moderate
+    e0 = B.Engine([B.System(n_big=nb, n_sml=ns, side=s.side, sigma_big=SB, sigma_sml=SS, dt=1e-5, seed=seed,
+                            T0=0.0, protocol="const", force_cap=50.0)])
+    e0.set_positions(pos)
+    e0.run(200)
+    start = e0.get_positions()[0]
+    e = B.Engine([s], neighbor_skin=SKIN)
+    e.set_positions(start)
+    e.run(1)
+    d = e.get_displacements()
+    ff, _, _, _, _ = O.eng_forces(start, types_of(s), s.side, SB, SS)
+    mob = np.where(types_of(s) == 0, np.float32(1) / np.float32(SB), np.float32(1) / np.float32(SS))
+    f_eng = d / (mob[:, None].astype(np.float64) * s.dt)
+    scale = np.abs(ff).max()
+    assert scale > 1.0
+    # float rounding of F mob dt and of the force sums (different pair order)
+    np.testing.assert_allclose(f_eng, ff.astype(np.float64), rtol=2e-5, atol=2e-5 * scale)
