@@ -133,11 +133,53 @@ struct ListBuild {
 // Lists of every home particle of each brick (grid-stride over bricks):
 // the staged sweep with the squared list cut distances (sigma + skin)^2,
 // partners recorded by storage id in sweep order.
+// Only the bricks of flagged replicas are visited: each block numbers them
+// (replica-major prefix of the flagged replicas' brick counts, in shared
+// memory) and takes every gridDim.x-th one, so no block walks the bricks of
+// unflagged replicas.
+constexpr int kSchedMaxRep = 1024;
 __global__ void __launch_bounds__(192, 4) k_list_build(StepArgs a, ListBuild lb) {
     extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_first[kSchedMaxRep + 1];  // flagged bricks before replica r
     if (lb.flag[lb.nrep] == 0) return;
     const int tid = threadIdx.x, T = blockDim.x;
-    for (int b = blockIdx.x; b < a.nbricks; b += gridDim.x) {
+    const int nrep = lb.nrep;
+    const bool sched = nrep <= kSchedMaxRep;
+    if (sched) {
+        for (int r = tid; r < nrep; r += T) {
+            const SysDev &S = a.sys[r];
+            s_first[r + 1] = lb.flag[r] ? S.nbx * S.nby * S.nbz : 0;
+        }
+        if (tid == 0) s_first[0] = 0;
+        __syncthreads();
+        if (tid < 32) {  // inclusive scan of s_first[1 .. nrep] by warp 0
+            int carry = 0;
+            for (int base = 1; base <= nrep; base += 32) {
+                const int i = base + tid;
+                int v = i <= nrep ? s_first[i] : 0;
+#pragma unroll
+                for (int off = 1; off < 32; off <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, v, off);
+                    if (tid >= off) v += y;
+                }
+                if (i <= nrep) s_first[i] = v + carry;
+                carry += __shfl_sync(0xffffffffu, v, 31);
+            }
+        }
+        __syncthreads();
+    }
+    const int total = sched ? s_first[nrep] : a.nbricks;
+    for (int w = blockIdx.x; w < total; w += gridDim.x) {
+        int b = w;
+        if (sched) {  // the replica with s_first[r] <= w < s_first[r + 1]
+            int lo = 0, hi = nrep - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (s_first[mid] <= w) lo = mid;
+                else hi = mid - 1;
+            }
+            b = a.sys[lo].brick_base + (w - s_first[lo]);
+        }
         const int4 br = a.bricks[b];
         if (lb.flag[br.x] == 0) continue;  // this replica's lists are still valid (uniform over the block)
         const SysDev &S = a.sys[br.x];
