@@ -264,10 +264,12 @@ int rebuild_grid(bd_engine *e, long long work) {
 // (e->lflag inside steps; e->d_one and null for observation passes).
 int list_bin(bd_engine *e, int cur, const int *any, const int *rflag) {
     cudaStream_t st = e->stream;
-    k_list_clear<<<rebuild_grid(e, div_up(e->C, 256)), 256, 0, st>>>(e->cnt[0], e->C, any);
+    // with rflag only the flagged replicas' cells are cleared and binned: a
+    // build stages cells of its own replica only
+    k_list_clear<<<rebuild_grid(e, div_up(e->C, 256)), 256, 0, st>>>(e->cnt[0], e->C, any, rflag, e->R, e->d_sys);
     k_list_bin<<<rebuild_grid(e, div_up(e->P, 256)), 256, 0, st>>>(e->lpos[cur & 1], (int)e->P, e->rep_of_sid,
                                                                  e->d_sys, e->cnt[0], e->pos[0], e->cap, e->status,
-                                                                 any, rflag);
+                                                                 any, rflag, e->R);
     BD_LAUNCH_CHECK();
     return BD_OK;
 }

@@ -92,32 +92,106 @@ __device__ __forceinline__ void st_state(T *p, T v) {
 }
 
 // ------------------------------------------------------------- rebuild
-__global__ void k_list_clear(int *cnt, long long C, const int *flag) {
+// Work over the flagged replicas only: s_first[r] = number of work items of
+// the flagged replicas before r (per replica: its particles, cells or
+// bricks), built in shared memory by the block; returns the total.
+constexpr int kSchedMaxRep = 1024;
+enum SchedItem { kItemParticle = 0, kItemCell = 1, kItemBrick = 2 };
+__device__ __forceinline__ int sched_count(const SysDev &S, int item) {
+    return item == kItemParticle ? S.n : item == kItemCell ? S.ncell * S.ncell * S.ncell : S.nbx * S.nby * S.nbz;
+}
+__device__ __forceinline__ int sched_first(const SysDev &S, int item) {
+    return item == kItemParticle ? S.part_base : item == kItemCell ? S.cell_base : S.brick_base;
+}
+__device__ int flagged_prefix(const int *__restrict__ rflag, int nrep, const SysDev *__restrict__ sys, int item,
+                              int *s_first) {
+    const int tid = threadIdx.x, T = blockDim.x;
+    for (int r = tid; r < nrep; r += T) s_first[r + 1] = rflag[r] ? sched_count(sys[r], item) : 0;
+    if (tid == 0) s_first[0] = 0;
+    __syncthreads();
+    if (tid < 32) {  // inclusive scan of s_first[1 .. nrep] by warp 0
+        int carry = 0;
+        for (int base = 1; base <= nrep; base += 32) {
+            const int i = base + tid;
+            int v = i <= nrep ? s_first[i] : 0;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, v, off);
+                if (tid >= off) v += y;
+            }
+            if (i <= nrep) s_first[i] = v + carry;
+            carry += __shfl_sync(0xffffffffu, v, 31);
+        }
+    }
+    __syncthreads();
+    return s_first[nrep];
+}
+// replica of work item w (s_first[r] <= w < s_first[r + 1]) and the item's
+// global index (storage id, cell or brick); the storage ids of a replica are
+// contiguous from its part_base
+__device__ __forceinline__ int sched_item(const int *s_first, int nrep, const SysDev *__restrict__ sys, int item,
+                                          int w, int *rep) {
+    int lo = 0, hi = nrep - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (s_first[mid] <= w) lo = mid;
+        else hi = mid - 1;
+    }
+    *rep = lo;
+    return sched_first(sys[lo], item) + (w - s_first[lo]);
+}
+
+// cell counts of the flagged replicas (all C cells when rflag is null)
+__global__ void k_list_clear(int *cnt, long long C, const int *flag, const int *rflag, int nrep, const SysDev *sys) {
+    __shared__ int s_first[kSchedMaxRep + 1];
     if (*flag == 0) return;
-    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < C; c += (long long)gridDim.x * blockDim.x)
-        cnt[c] = 0;
+    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x, nt = (long long)gridDim.x * blockDim.x;
+    if (rflag && nrep <= kSchedMaxRep) {
+        const int total = flagged_prefix(rflag, nrep, sys, kItemCell, s_first);
+        for (long long w = t0; w < total; w += nt) {
+            int r;
+            cnt[sched_item(s_first, nrep, sys, kItemCell, (int)w, &r)] = 0;
+        }
+        return;
+    }
+    for (long long c = t0; c < C; c += nt) cnt[c] = 0;
+}
+
+__device__ __forceinline__ void bin_particle(const float4 *__restrict__ pos_sid, int sid, const SysDev &S, int *cnt,
+                                             float4 *pos, int cap, unsigned *status) {
+    const float4 v = pos_sid[sid];
+    const int nc = S.ncell;
+    int ix = (int)__fmul_rn(v.x, S.cinv), iy = (int)__fmul_rn(v.y, S.cinv), iz = (int)__fmul_rn(v.z, S.cinv);
+    ix = min(max(ix, 0), nc - 1);
+    iy = min(max(iy, 0), nc - 1);
+    iz = min(max(iz, 0), nc - 1);
+    const int cell = S.cell_base + ix + nc * (iy + nc * iz);
+    const int slot = atomicAdd(cnt + cell, 1);
+    if (slot < cap) pos[(size_t)cell * cap + slot] = v;
+    else set_status(status, kStatCellOverflow);
 }
 
 // cell buckets from the by-id positions (same binning as the step kernels)
 // of the replicas whose flag is set (every replica when rflag is null)
 __global__ void k_list_bin(const float4 *__restrict__ pos_sid, int P, const int *__restrict__ rep_of_sid,
                            const SysDev *sys, int *cnt, float4 *pos, int cap, unsigned *status, const int *flag,
-                           const int *rflag) {
+                           const int *rflag, int nrep) {
+    __shared__ int s_first[kSchedMaxRep + 1];
     if (*flag == 0) return;
-    for (int sid = blockIdx.x * blockDim.x + threadIdx.x; sid < P; sid += gridDim.x * blockDim.x) {
+    const int t0 = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
+    if (rflag && nrep <= kSchedMaxRep) {
+        const int total = flagged_prefix(rflag, nrep, sys, kItemParticle, s_first);
+        for (int w = t0; w < total; w += nt) {
+            int r;
+            const int sid = sched_item(s_first, nrep, sys, kItemParticle, w, &r);
+            bin_particle(pos_sid, sid, sys[r], cnt, pos, cap, status);
+        }
+        return;
+    }
+    for (int sid = t0; sid < P; sid += nt) {
         const int r = rep_of_sid[sid];
         if (rflag && rflag[r] == 0) continue;
-        const float4 v = pos_sid[sid];
-        const SysDev &S = sys[r];
-        const int nc = S.ncell;
-        int ix = (int)__fmul_rn(v.x, S.cinv), iy = (int)__fmul_rn(v.y, S.cinv), iz = (int)__fmul_rn(v.z, S.cinv);
-        ix = min(max(ix, 0), nc - 1);
-        iy = min(max(iy, 0), nc - 1);
-        iz = min(max(iz, 0), nc - 1);
-        const int cell = S.cell_base + ix + nc * (iy + nc * iz);
-        const int slot = atomicAdd(cnt + cell, 1);
-        if (slot < cap) pos[(size_t)cell * cap + slot] = v;
-        else set_status(status, kStatCellOverflow);
+        bin_particle(pos_sid, sid, sys[r], cnt, pos, cap, status);
     }
 }
 
@@ -134,52 +208,19 @@ struct ListBuild {
 // the staged sweep with the squared list cut distances (sigma + skin)^2,
 // partners recorded by storage id in sweep order.
 // Only the bricks of flagged replicas are visited: each block numbers them
-// (replica-major prefix of the flagged replicas' brick counts, in shared
-// memory) and takes every gridDim.x-th one, so no block walks the bricks of
-// unflagged replicas.
-constexpr int kSchedMaxRep = 1024;
+// (flagged_prefix) and takes every gridDim.x-th one, so no block walks the
+// bricks of unflagged replicas.
 __global__ void __launch_bounds__(192, 4) k_list_build(StepArgs a, ListBuild lb) {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ int s_first[kSchedMaxRep + 1];  // flagged bricks before replica r
+    __shared__ int s_first[kSchedMaxRep + 1];
     if (lb.flag[lb.nrep] == 0) return;
     const int tid = threadIdx.x, T = blockDim.x;
     const int nrep = lb.nrep;
     const bool sched = nrep <= kSchedMaxRep;
-    if (sched) {
-        for (int r = tid; r < nrep; r += T) {
-            const SysDev &S = a.sys[r];
-            s_first[r + 1] = lb.flag[r] ? S.nbx * S.nby * S.nbz : 0;
-        }
-        if (tid == 0) s_first[0] = 0;
-        __syncthreads();
-        if (tid < 32) {  // inclusive scan of s_first[1 .. nrep] by warp 0
-            int carry = 0;
-            for (int base = 1; base <= nrep; base += 32) {
-                const int i = base + tid;
-                int v = i <= nrep ? s_first[i] : 0;
-#pragma unroll
-                for (int off = 1; off < 32; off <<= 1) {
-                    const int y = __shfl_up_sync(0xffffffffu, v, off);
-                    if (tid >= off) v += y;
-                }
-                if (i <= nrep) s_first[i] = v + carry;
-                carry += __shfl_sync(0xffffffffu, v, 31);
-            }
-        }
-        __syncthreads();
-    }
-    const int total = sched ? s_first[nrep] : a.nbricks;
+    const int total = sched ? flagged_prefix(lb.flag, nrep, a.sys, kItemBrick, s_first) : a.nbricks;
     for (int w = blockIdx.x; w < total; w += gridDim.x) {
-        int b = w;
-        if (sched) {  // the replica with s_first[r] <= w < s_first[r + 1]
-            int lo = 0, hi = nrep - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (s_first[mid] <= w) lo = mid;
-                else hi = mid - 1;
-            }
-            b = a.sys[lo].brick_base + (w - s_first[lo]);
-        }
+        int r;
+        const int b = sched ? sched_item(s_first, nrep, a.sys, kItemBrick, w, &r) : w;
         const int4 br = a.bricks[b];
         if (lb.flag[br.x] == 0) continue;  // this replica's lists are still valid (uniform over the block)
         const SysDev &S = a.sys[br.x];
