@@ -9,11 +9,17 @@
 // A CTA owns a brick of kGrBrick^3 cells (its "home" particles) and sweeps
 // every cell within m = ceil(range / cell side) cells of the brick in tiles
 // of kGrTileCells cells, skipping cells whose nearest point lies farther than
-// `range` from the brick.  Each (home, candidate) ordered pair is binned with
-// the reference's rounding; counts go to a shared-memory histogram and then
-// to 64-bit global counters, so the result is the exact integer histogram of
-// the all-pairs kernel.  The candidate region (kGrBrick + 2m cells per axis)
-// must not wrap onto itself, so every cell appears at most once.
+// `range` from the brick.  Every unordered pair is evaluated once: a
+// candidate counts when its brick comes after the home brick in brick order,
+// and within the home brick when its storage id is larger; the pair then adds
+// one count to each of its two ordered bins (two to one bin for equal
+// species).  Inside the range the minimum-image distance of (j, i) is the
+// exact negation of that of (i, j), so the ordered counts are those of the
+// reference.  Bins use the reference's rounding; counts go to a shared-memory
+// histogram and then to 64-bit global counters, so the result is the exact
+// integer histogram of the all-pairs kernel.  The candidate region
+// (kGrBrick + 2m cells per axis) must not wrap onto itself, so every cell
+// appears at most once.
 //
 // The bound assumes every particle lies in its cell to within
 // kGrTol * cell side.  The engine's wrap keeps positions in [0, L], but a
@@ -89,6 +95,29 @@ __device__ int gr_scan(int *a, int n, int *wsum) {
 }
 
 // last index c in [0, n) with start[c] <= t
+// one unordered pair (i, j) within range: both ordered counts
+__device__ __forceinline__ void gr_count_pair(float4 pi, float4 pj, float side, float side_inv, float range,
+                                              float range2_hi, float bin_size, int nbins, unsigned *hist) {
+    const float dx = min_image_gder_fast(__fsub_rn(pi.x, pj.x), side, side_inv);
+    const float dy = min_image_gder_fast(__fsub_rn(pi.y, pj.y), side, side_inv);
+    const float dz = min_image_gder_fast(__fsub_rn(pi.z, pj.z), side, side_inv);
+    const float d2 = dist2_rn(dx, dy, dz);
+    if (d2 <= range2_hi) {
+        const float dist = __fsqrt_rn(d2);
+        if (dist < range) {
+            int bin = (int)__fdiv_rn(dist, bin_size);
+            if (bin == nbins) bin--;
+            const unsigned ti = __float_as_uint(pi.w) >> 31, tj = __float_as_uint(pj.w) >> 31;
+            if (ti == tj) {
+                atomicAdd(&hist[3 * ti * nbins + bin], 2u);
+            } else {
+                atomicAdd(&hist[(2 * ti + tj) * nbins + bin], 1u);
+                atomicAdd(&hist[(2 * tj + ti) * nbins + bin], 1u);
+            }
+        }
+    }
+}
+
 __device__ __forceinline__ int gr_find(const int *start, int n, int t) {
     int lo = 0, hi = n - 1;
     while (lo < hi) {
@@ -156,7 +185,24 @@ __global__ void __launch_bounds__(kGrThreads) k_gr_cells(GrArgs a) {
     }
 
     if (H > 0) {
-        // 2. candidate region, tile by tile
+        // 2. pairs inside the home brick, each once (smaller storage id first)
+        {
+            const int nhh = H * H;
+            int h = tid % H, c = tid / H;
+            const int dh = kGrThreads % H, dc = kGrThreads / H;
+            for (int p = tid; p < nhh; p += kGrThreads) {
+                const float4 pi = home[h], pj = home[c];
+                if ((__float_as_uint(pi.w) & 0x7fffffffu) < (__float_as_uint(pj.w) & 0x7fffffffu))
+                    gr_count_pair(pi, pj, side, side_inv, range, range2_hi, bin_size, nbins, hist);
+                h += dh;
+                c += dc;
+                if (h >= H) { h -= H; c++; }
+            }
+        }
+        // 3. candidate region, tile by tile: only cells of bricks after the
+        // home brick (brick order of the grid this kernel tiles with)
+        const int nbr = (nc + kGrBrick - 1) / kGrBrick;
+        const int hb = ox / kGrBrick + nbr * (oy / kGrBrick + nbr * (oz / kGrBrick));
         const int rx = wx + 2 * m, ry = wy + 2 * m, rz = wz + 2 * m;
         const int nreg = rx * ry * rz;
         const int dh = kGrThreads % H, dc = kGrThreads / H;
@@ -176,7 +222,8 @@ __global__ void __launch_bounds__(kGrThreads) k_gr_cells(GrArgs a) {
                     gy += gy < 0 ? nc : 0; gy -= gy >= nc ? nc : 0;
                     gz += gz < 0 ? nc : 0; gz -= gz >= nc ? nc : 0;
                     gc = S.cell_base + gx + nc * (gy + nc * gz);
-                    k = min(max(a.cnt[gc], 0), a.cap);
+                    const int cb = gx / kGrBrick + nbr * (gy / kGrBrick + nbr * (gz / kGrBrick));
+                    if (cb > hb) k = min(max(a.cnt[gc], 0), a.cap);
                 }
                 cstart[q] = k;
                 cgc[q] = gc;
@@ -190,26 +237,11 @@ __global__ void __launch_bounds__(kGrThreads) k_gr_cells(GrArgs a) {
                 tile[t] = a.pos[(size_t)cgc[c] * a.cap + (t - cstart[c])];
             }
             __syncthreads();
-            // ordered pairs (home h, candidate c), h fastest
+            // pairs (home h, candidate c) of different bricks, h fastest
             const int np = H * Tn;
             int h = tid % H, c = tid / H;
             for (int p = tid; p < np; p += kGrThreads) {
-                const float4 pi = home[h], pj = tile[c];
-                const unsigned wi = __float_as_uint(pi.w), wj = __float_as_uint(pj.w);
-                if ((wi & 0x7fffffffu) != (wj & 0x7fffffffu)) {
-                    const float dx = min_image_gder_fast(__fsub_rn(pi.x, pj.x), side, side_inv);
-                    const float dy = min_image_gder_fast(__fsub_rn(pi.y, pj.y), side, side_inv);
-                    const float dz = min_image_gder_fast(__fsub_rn(pi.z, pj.z), side, side_inv);
-                    const float d2 = dist2_rn(dx, dy, dz);
-                    if (d2 <= range2_hi) {
-                        const float dist = __fsqrt_rn(d2);
-                        if (dist < range) {
-                            int bin = (int)__fdiv_rn(dist, bin_size);
-                            if (bin == nbins) bin--;
-                            atomicAdd(&hist[((wi >> 31) * 2 + (wj >> 31)) * nbins + bin], 1u);
-                        }
-                    }
-                }
+                gr_count_pair(home[h], tile[c], side, side_inv, range, range2_hi, bin_size, nbins, hist);
                 h += dh;
                 c += dc;
                 if (h >= H) { h -= H; c++; }
