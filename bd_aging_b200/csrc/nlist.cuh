@@ -34,9 +34,6 @@ constexpr int kMaxNbr = 64;
 #ifndef BD_LIST_MINB
 #define BD_LIST_MINB 4       // resident CTAs per SM asked of the register allocator (64 registers)
 #endif
-#ifndef BD_LIST_STREAM
-#define BD_LIST_STREAM 0     // evict-first loads/stores: 1 per-particle state, 2 also list words
-#endif
 constexpr int kGather = BD_LIST_GATHER;
 static_assert(kGather % 2 == 0 && kMaxNbr % kGather == 0, "partners are paired for f32x2 arithmetic");
 
@@ -70,25 +67,6 @@ struct ListArgs {
 // shortcut when |d / L| < 0.49
 __device__ __forceinline__ float min_image_fast(float d, float L, float Linv) {
     return fabsf(__fmul_rn(Linv, d)) < 0.49f ? d : min_image_f(d, L, Linv);
-}
-
-// Per-particle state is touched once per step: with BD_LIST_STREAM its loads
-// and stores take the evict-first policy, so the positions that the partner
-// gathers read stay in L2.
-template <int LEVEL, class T>
-__device__ __forceinline__ T ld_state(const T *p) {
-    if (BD_LIST_STREAM >= LEVEL) return __ldcs(p);
-    return __ldg(p);
-}
-template <class T>
-__device__ __forceinline__ T ld_state_rw(const T *p) {  // read and written by the same thread
-    if (BD_LIST_STREAM >= 1) return __ldcs(p);
-    return *p;
-}
-template <class T>
-__device__ __forceinline__ void st_state(T *p, T v) {
-    if (BD_LIST_STREAM >= 1) __stcs(p, v);
-    else *p = v;
 }
 
 // ------------------------------------------------------------- rebuild
@@ -307,7 +285,7 @@ __global__ void k_list_done(int *flag, int nrep, long long *builds) {
 // list words k0 .. k0 + kGather - 1 (k0 < kMaxNbr)
 __device__ __forceinline__ void list_words(const ListArgs &a, int sid, int k0, int (&jn)[kGather]) {
 #pragma unroll
-    for (int u = 0; u < kGather; u++) jn[u] = ld_state<2>(a.nbr + (size_t)(k0 + u) * a.np + sid);
+    for (int u = 0; u < kGather; u++) jn[u] = __ldg(a.nbr + (size_t)(k0 + u) * a.np + sid);
 }
 // positions of the chunk's partners: an entry outside [0, np) reads the zero
 // position at np and counts as absent (jj = np)
@@ -445,11 +423,11 @@ __global__ void __launch_bounds__(BD_LIST_THREADS, BD_LIST_MINB) k_step_list(Lis
     const float sg0 = tm ? S.sig[1] : S.sig[0], sg1 = tm ? S.sig[2] : S.sig[1];
     const float c0 = tm ? S.cut2[1] : S.cut2[0], c1 = tm ? S.cut2[2] : S.cut2[1];
     // own state early: its latency overlaps the force loop
-    const int gid = ld_state<1>(a.gid_of + sid);
-    float lx = ld_state_rw(a.lo_x + sid), ly = ld_state_rw(a.lo_y + sid), lz = ld_state_rw(a.lo_z + sid);
-    const float4 pb = ld_state<1>(a.pbuild + sid);
+    const int gid = __ldg(a.gid_of + sid);
+    float lx = a.lo_x[sid], ly = a.lo_y[sid], lz = a.lo_z[sid];
+    const float4 pb = __ldg(a.pbuild + sid);
     float fx, fy, fz;
-    const int n = min(ld_state<1>(a.nnb + sid), kMaxNbr);
+    const int n = min(__ldg(a.nnb + sid), kMaxNbr);
     if (EXTRA && S.pot != kPotWcaModified) {
         list_forces_extra(a, S, sid, n, pi, tm, fx, fy, fz);
     } else {  // the same arithmetic in either instantiation: a replica's result does not depend on its batch
@@ -513,9 +491,9 @@ __global__ void __launch_bounds__(BD_LIST_THREADS, BD_LIST_MINB) k_step_list(Lis
     if (kx != 0.f) a.img[sid] += (int)kx;
     if (ky != 0.f) a.img[a.np + sid] += (int)ky;
     if (kz != 0.f) a.img[2 * a.np + sid] += (int)kz;
-    st_state(a.lo_x + sid, lx);
-    st_state(a.lo_y + sid, ly);
-    st_state(a.lo_z + sid, lz);
+    a.lo_x[sid] = lx;
+    a.lo_y[sid] = ly;
+    a.lo_z[sid] = lz;
     if (!(isfinite(x) && isfinite(y) && isfinite(z))) set_status(a.status, kStatNumeric);
     a.pos_out[sid] = make_float4(x, y, z, pi.w);
     // skin check against the positions at the last build
