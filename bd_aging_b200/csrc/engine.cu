@@ -204,7 +204,7 @@ int configure_kernels(bd_engine *e) {
     BD_ATTR(kRngNoise)
     BD_ATTR(kRngRannew64)
 #undef BD_ATTR
-    if (cudaFuncSetAttribute(k_list_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e->smem) != cudaSuccess)
+    if (cudaFuncSetAttribute(k_list_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e->lsmem) != cudaSuccess)
         rc = 1;
     return rc ? BD_ERR_CUDA : BD_OK;
 }
@@ -281,7 +281,7 @@ int list_rebuild(bd_engine *e, int cur) {
     int rc = list_bin(e, cur, e->lflag + e->R, e->lflag);
     if (rc) return rc;
     ListBuild lb{e->nbr, e->nnb, e->pbuild, e->lpos[cur & 1], e->lflag, e->R};
-    k_list_build<<<rebuild_grid(e, e->nbricks), e->threads, e->smem, st>>>(make_args(e, 0, 0), lb);
+    k_list_build<<<rebuild_grid(e, e->nbricks), kListBuildThreads, e->lsmem, st>>>(make_args(e, 0, 0), lb);
     k_list_done<<<1, 256, 0, st>>>(e->lflag, e->R, e->d_builds);
     BD_LAUNCH_CHECK();
     return BD_OK;
@@ -427,7 +427,8 @@ int rebuild_bricks(bd_engine *e) {
     e->smax = (int)std::min<long long>(std::min<long long>(65534, (long long)nh * e->cap), std::max(256LL, want)) & ~1;
     e->smem = brick_smem_bytes(nh, e->smax, e->threads);
     e->smem_census = e->smem;
-    if (e->smem > 227 * 1024 || nh > 65535) return BD_ERR_ARG;
+    e->lsmem = brick_smem_bytes(nh, e->smax, kListBuildThreads);
+    if (e->smem > 227 * 1024 || e->lsmem > 227 * 1024 || nh > 65535) return BD_ERR_ARG;
     e->cl_start_h.clear();
     e->cl_bricks_h.clear();
     if (e->mode == BD_MODE_PERSISTENT) {

@@ -22,6 +22,7 @@ struct bd_engine {
     int nbricks = 0;
     int bx = 4, by = 4, bz = 3, cap = 16, threads = 128, smax = 0, mode = BD_MODE_PLAIN, cluster = 8;
     size_t smem = 0, smem_census = 0;
+    size_t lsmem = 0;  // list build (kListBuildThreads per CTA)
     long long C = 0, P = 0;
     int *cnt[3] = {nullptr, nullptr, nullptr};
     float4 *pos[3] = {nullptr, nullptr, nullptr};

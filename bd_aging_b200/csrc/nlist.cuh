@@ -35,6 +35,7 @@ constexpr int kMaxNbr = 64;
 #define BD_LIST_MINB 4       // resident CTAs per SM asked of the register allocator (64 registers)
 #endif
 constexpr int kGather = BD_LIST_GATHER;
+constexpr int kListBuildThreads = 256;  // CTA size of the list build
 static_assert(kGather % 2 == 0 && kMaxNbr % kGather == 0, "partners are paired for f32x2 arithmetic");
 
 struct ListArgs {
@@ -188,7 +189,11 @@ struct ListBuild {
 // Only the bricks of flagged replicas are visited: each block numbers them
 // (flagged_prefix) and takes every gridDim.x-th one, so no block walks the
 // bricks of unflagged replicas.
-__global__ void __launch_bounds__(192, 4) k_list_build(StepArgs a, ListBuild lb) {
+// One thread per home particle of a brick in one round (a brick holds about
+// 170 particles at phi = 0.58): a rebuild of a few replicas runs one brick
+// per SM, so its time is one CTA's staging plus one particle's sweep.  The
+// lists do not depend on the CTA size (each particle's sweep order is fixed).
+__global__ void __launch_bounds__(kListBuildThreads, 2) k_list_build(StepArgs a, ListBuild lb) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_first[kSchedMaxRep + 1];
     if (lb.flag[lb.nrep] == 0) return;
