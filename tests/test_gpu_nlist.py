@@ -218,3 +218,33 @@ def test_list_forces_match_oracle_at_zero_temperature(nb, ns, phi, seed):
     assert scale > 1.0
     # float rounding of F mob dt and of the force sums (different pair order)
     np.testing.assert_allclose(f_eng, ff.astype(np.float64), rtol=2e-5, atol=2e-5 * scale)
+
+
+def test_many_replicas_rebuild_only_the_flagged_ones():
+    # 40 replicas (the rebuild kernels number the flagged replicas' particles,
+    # cells and bricks with a scan over replicas, here over two warp chunks):
+    # hot ones rebuild often, cold ones rarely.  Each replica ends bit-identical
+    # to its own single-replica run, and every neighbour set is exact.
+    temps = [2.0 if k % 3 == 0 else 1e-3 for k in range(40)]
+    specs = [(60 + 7 * k, 90 - k, 0.45, 100 + k) for k in range(40)]
+    systems, poss = zip(*[system(*sp, T0=t, protocol="const", dt=2e-4) for sp, t in zip(specs, temps)])
+    eb = B.Engine(list(systems), neighbor_skin=SKIN)
+    eb.set_positions(np.concatenate(poss))
+    eb.run(120)
+    pb, rb = eb.get_positions()
+    assert eb.info().list_builds > 40 + 10  # the first builds plus hot-replica rebuilds
+    cnt, hsh = eb.census()
+    for k in (0, 1, 17, 39):
+        s = systems[k]
+        e1 = B.Engine([s], neighbor_skin=SKIN)
+        e1.set_positions(poss[k])
+        e1.run(120)
+        p1, r1 = e1.get_positions()
+        sl = slice(eb.offsets[k], eb.offsets[k + 1])
+        np.testing.assert_array_equal(pb[sl], p1)
+        np.testing.assert_array_equal(rb[sl], r1)
+    for k, s in enumerate(systems):
+        sl = slice(eb.offsets[k], eb.offsets[k + 1])
+        _, _, _, nbr, h = O.eng_forces(pb[sl], types_of(s), s.side, SB, SS)
+        np.testing.assert_array_equal(cnt[sl], nbr)
+        np.testing.assert_array_equal(hsh[sl], h)
