@@ -27,12 +27,19 @@ __device__ __forceinline__ int gr_bin(float dx, float dy, float dz, float side, 
     if (bin == nbins) bin--;
     return bin;
 }
+// Histogram: with `per_warp` every warp adds into its own copy in shared
+// memory with plain atomics (bins spread over the warp's lanes rarely
+// collide), and the copies are summed at the end; otherwise one copy per
+// block, with lanes of equal bins combined by __match_any_sync first.
 __global__ void __launch_bounds__(256) k_gr_batch(const float4 *__restrict__ snap, int n, int n_big, float side,
-                                                  float range, int nbins, int jchunk, unsigned long long *counts) {
+                                                  float range, int nbins, int jchunk, int per_warp,
+                                                  unsigned long long *counts) {
     extern __shared__ __align__(16) unsigned char smem[];
     float4 *tile = reinterpret_cast<float4 *>(smem);
-    unsigned *hist = reinterpret_cast<unsigned *>(tile + kGrTile);  // [4][nbins]
-    for (int b = threadIdx.x; b < 4 * nbins; b += blockDim.x) hist[b] = 0;
+    unsigned *hist0 = reinterpret_cast<unsigned *>(tile + kGrTile);  // [copies][4][nbins]
+    const int nw = blockDim.x / 32, copies = per_warp ? nw : 1;
+    for (int b = threadIdx.x; b < copies * 4 * nbins; b += blockDim.x) hist0[b] = 0;
+    unsigned *hist = hist0 + (per_warp ? (threadIdx.x >> 5) * 4 * nbins : 0);
     const float side_inv = __double2float_rn(1.0 / (double)side);
     const float bin_size = __fdiv_rn(range, (float)nbins);
     const float range2_hi = range * range * 1.00001f;
@@ -55,21 +62,31 @@ __global__ void __launch_bounds__(256) k_gr_batch(const float4 *__restrict__ sna
                 float4 pj = tile[t];
                 float dx = __fsub_rn(pi.x, pj.x), dy = __fsub_rn(pi.y, pj.y), dz = __fsub_rn(pi.z, pj.z);
                 int bf = gr_bin(dx, dy, dz, side, side_inv, range, range2_hi, bin_size, nbins);
-                bool sym = fabsf(__fmul_rn(side_inv, dx)) < 0.25f && fabsf(__fmul_rn(side_inv, dy)) < 0.25f &&
-                           fabsf(__fmul_rn(side_inv, dz)) < 0.25f;
+                // below 0.49 the minimum image returns d itself for both signs
+                // (min_image_gder_fast), so the reverse distance is the same
+                bool sym = fabsf(__fmul_rn(side_inv, dx)) < 0.49f && fabsf(__fmul_rn(side_inv, dy)) < 0.49f &&
+                           fabsf(__fmul_rn(side_inv, dz)) < 0.49f;
                 int bb = sym ? bf : gr_bin(-dx, -dy, -dz, side, side_inv, range, range2_hi, bin_size, nbins);
                 if (bf >= 0) kf = (ti * 2 + tj) * nbins + bf;
                 if (bb >= 0) kr = (tj * 2 + ti) * nbins + bb;
             }
-            unsigned s1 = __match_any_sync(0xffffffffu, kf);
-            if (kf >= 0 && (threadIdx.x & 31) == __ffs(s1) - 1) atomicAdd(&hist[kf], (unsigned)__popc(s1));
-            unsigned s2 = __match_any_sync(0xffffffffu, kr);
-            if (kr >= 0 && (threadIdx.x & 31) == __ffs(s2) - 1) atomicAdd(&hist[kr], (unsigned)__popc(s2));
+            if (per_warp) {
+                if (kf >= 0) atomicAdd(&hist[kf], 1u);
+                if (kr >= 0) atomicAdd(&hist[kr], 1u);
+            } else {
+                unsigned s1 = __match_any_sync(0xffffffffu, kf);
+                if (kf >= 0 && (threadIdx.x & 31) == __ffs(s1) - 1) atomicAdd(&hist[kf], (unsigned)__popc(s1));
+                unsigned s2 = __match_any_sync(0xffffffffu, kr);
+                if (kr >= 0 && (threadIdx.x & 31) == __ffs(s2) - 1) atomicAdd(&hist[kr], (unsigned)__popc(s2));
+            }
         }
     }
     __syncthreads();
-    for (int b = threadIdx.x; b < 4 * nbins; b += blockDim.x)
-        if (hist[b]) atomicAdd(&counts[b], (unsigned long long)hist[b]);
+    for (int b = threadIdx.x; b < 4 * nbins; b += blockDim.x) {
+        unsigned long long v = 0;
+        for (int c = 0; c < copies; c++) v += hist0[c * 4 * nbins + b];
+        if (v) atomicAdd(&counts[b], v);
+    }
 }
 
 }  // namespace bd
@@ -994,7 +1011,9 @@ int bd_engine_gder_method(bd_engine *e, int nbins, float range, int method, unsi
         k_export<<<div_up(e->C, 128), 128, 0, e->stream>>>(e->cnt[obs_buf(e)], e->pos[obs_buf(e)], (int)e->C, e->cap, (int)e->P,
                                                            e->gid_of, e->x0, e->dsp[0], e->dsp[1], e->dsp[2], nullptr,
                                                            nullptr, e->snap);
-        const size_t sm = kGrTile * sizeof(float4) + per * sizeof(unsigned);
+        // one histogram copy per warp when 8 of them fit beside the tile
+        const int per_warp = (size_t)8 * per * sizeof(unsigned) <= 160 * 1024 ? 1 : 0;
+        const size_t sm = kGrTile * sizeof(float4) + (per_warp ? 8 : 1) * per * sizeof(unsigned);
         cudaFuncSetAttribute(k_gr_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         const int jchunk = 8192;
         for (int r = 0; r < e->R; r++) {
@@ -1002,7 +1021,7 @@ int bd_engine_gder_method(bd_engine *e, int nbins, float range, int method, unsi
             const SysDev &S = e->sysh[r];
             dim3 grid(div_up(S.n, 256), div_up(S.n, jchunk));
             k_gr_batch<<<grid, 256, sm, e->stream>>>(e->snap + S.part_base, S.n, S.n_big, S.L, range, nbins, jchunk,
-                                                     d_counts + per * r);
+                                                     per_warp, d_counts + per * r);
         }
         le = cudaGetLastError();
         if (le != cudaSuccess) rc = BD_ERR_CUDA;
