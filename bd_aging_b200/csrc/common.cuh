@@ -47,6 +47,29 @@ __device__ __forceinline__ float min_image_gder(float d, float side, float side_
 __device__ __forceinline__ float min_image_gder_fast(float d, float side, float side_inv) {
     return fabsf(__fmul_rn(side_inv, d)) < 0.49f ? d : min_image_gder(d, side, side_inv);
 }
+// ---------------------------------------------------------------- g(r) bins
+// The reference bins a pair at (int)(dist / bin_size) with dist =
+// sqrt(d2) (get_gder.cu:116-121), both correctly rounded, when dist < range;
+// a bin equal to nbins (rounding at the range) goes to the last bin.  That
+// bin is a non-decreasing function of d2, so it is fixed by thresholds:
+// gr_thr[k] = the smallest float d2 whose bin is >= k (k = 1 .. nbins), and
+// gr_thr[nbins + 1] = the smallest d2 with dist >= range.  Found once per
+// call by bisection over the bit patterns of non-negative floats
+// (k_gr_thresholds in engine.cu).
+__device__ __forceinline__ int gr_bin_exact(float d2, float bin_size) {
+    return (int)__fdiv_rn(__fsqrt_rn(d2), bin_size);
+}
+// bin of d2 (-1 outside the range) from the thresholds in shared memory: a
+// fast estimate (off by at most one) corrected against them
+__device__ __forceinline__ int gr_bin_thr(float d2, const float *thr, float inv_bin_size, int nbins) {
+    if (!(d2 < thr[nbins + 1])) return -1;
+    int b = (int)fmaxf(0.f, __fmul_rn(__fmul_rn(d2, rsqrtf(d2)), inv_bin_size));
+    b = min(b, nbins);
+    if (b < nbins && d2 >= thr[b + 1]) b++;
+    else if (b > 0 && d2 < thr[b]) b--;
+    return min(b, nbins - 1);
+}
+
 // (dx*dx + dy*dy) + dz*dz, every operation rounded (reference host order)
 __device__ __forceinline__ float dist2_rn(float dx, float dy, float dz) {
     return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));

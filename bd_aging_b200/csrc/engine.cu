@@ -13,41 +13,61 @@ namespace bd {
 // type_i), recomputed when the minimum-image rounding can differ.  Big
 // particles come first, so i < j gives bb, bs and ss forward and bb, sb, ss
 // in reverse.
+// g(r) bin thresholds (gr_bin_thr): thr[k], k = 0 .. nbins + 1
+__global__ void k_gr_thresholds(float range, int nbins, float *thr) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > nbins + 1) return;
+    if (k == 0) { thr[0] = 0.f; return; }
+    const float bin_size = __fdiv_rn(range, (float)nbins);
+    unsigned lo = 0u, hi = 0x7f800000u;  // +0 .. +inf
+    while (lo < hi) {
+        const unsigned mid = lo + ((hi - lo) >> 1);
+        const float x = __uint_as_float(mid);
+        const bool reach = k <= nbins ? gr_bin_exact(x, bin_size) >= k : !(__fsqrt_rn(x) < range);
+        if (reach) hi = mid;
+        else lo = mid + 1;
+    }
+    thr[k] = __uint_as_float(lo);
+}
 constexpr int kGrTile = 1024;
-__device__ __forceinline__ int gr_bin(float dx, float dy, float dz, float side, float side_inv, float range,
-                                      float range2_hi, float bin_size, int nbins) {
+__device__ __forceinline__ int gr_bin(float dx, float dy, float dz, float side, float side_inv, const float *thr,
+                                      float inv_bin_size, int nbins) {
     dx = min_image_gder_fast(dx, side, side_inv);
     dy = min_image_gder_fast(dy, side, side_inv);
     dz = min_image_gder_fast(dz, side, side_inv);
-    float d2 = dist2_rn(dx, dy, dz);
-    if (!(d2 <= range2_hi)) return -1;
-    float dist = __fsqrt_rn(d2);
-    if (!(dist < range)) return -1;
-    int bin = (int)__fdiv_rn(dist, bin_size);
-    if (bin == nbins) bin--;
-    return bin;
+    return gr_bin_thr(dist2_rn(dx, dy, dz), thr, inv_bin_size, nbins);
 }
-// Histogram: with `per_warp` every warp adds into its own copy in shared
-// memory with plain atomics (bins spread over the warp's lanes rarely
-// collide), and the copies are summed at the end; otherwise one copy per
-// block, with lanes of equal bins combined by __match_any_sync first.
-__global__ void __launch_bounds__(256) k_gr_batch(const float4 *__restrict__ snap, int n, int n_big, float side,
-                                                  float range, int nbins, int jchunk, int per_warp,
-                                                  unsigned long long *counts) {
+// One launch for every replica that needs all pairs (blockIdx.z indexes
+// `reps`).  Histogram: with `copies` > 1 each pair of warps adds into its own
+// copy in shared memory with plain atomics (bins spread over the lanes rarely
+// collide), and the copies are summed at the end; with one copy, lanes of
+// equal bins are combined by __match_any_sync first.
+__global__ void __launch_bounds__(256) k_gr_batch(const float4 *__restrict__ snap_all, const SysDev *__restrict__ sys,
+                                                  const int *__restrict__ reps, float range,
+                                                  const float *__restrict__ thr_g, int nbins, int jchunk, int copies,
+                                                  unsigned long long *counts_all) {
     extern __shared__ __align__(16) unsigned char smem[];
+    const int r = reps[blockIdx.z];
+    const SysDev &S = sys[r];
+    const int n = S.n, n_big = S.n_big;
+    const int j0 = max(blockIdx.y * jchunk, (int)(blockIdx.x * blockDim.x) + 1), j1 = min(n, (int)(blockIdx.y + 1) * jchunk);
+    if (j0 >= j1) return;  // uniform over the block: no pair of this replica here
+    const float4 *snap = snap_all + S.part_base;
+    unsigned long long *counts = counts_all + (size_t)r * 4 * nbins;
+    const float side = S.L;
     float4 *tile = reinterpret_cast<float4 *>(smem);
-    unsigned *hist0 = reinterpret_cast<unsigned *>(tile + kGrTile);  // [copies][4][nbins]
-    const int nw = blockDim.x / 32, copies = per_warp ? nw : 1;
+    float *thr = reinterpret_cast<float *>(tile + kGrTile);          // [nbins + 2] bin thresholds
+    unsigned *hist0 = reinterpret_cast<unsigned *>(thr + nbins + 2);  // [copies][4][nbins]
     for (int b = threadIdx.x; b < copies * 4 * nbins; b += blockDim.x) hist0[b] = 0;
-    unsigned *hist = hist0 + (per_warp ? (threadIdx.x >> 5) * 4 * nbins : 0);
+    for (int b = threadIdx.x; b < nbins + 2; b += blockDim.x) thr[b] = thr_g[b];
+    const int per_copy = (blockDim.x / 32 + copies - 1) / copies;  // warps per copy
+    unsigned *hist = hist0 + ((threadIdx.x >> 5) / per_copy) * 4 * nbins;
     const float side_inv = __double2float_rn(1.0 / (double)side);
-    const float bin_size = __fdiv_rn(range, (float)nbins);
-    const float range2_hi = range * range * 1.00001f;
+    const float inv_bin_size = 1.0f / __fdiv_rn(range, (float)nbins);  // estimate only (gr_bin_thr)
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool vi = i < n;
     float4 pi = vi ? snap[i] : make_float4(0, 0, 0, 0);
     const int ti = i < n_big ? 0 : 1;
-    int j0 = max(blockIdx.y * jchunk, (int)(blockIdx.x * blockDim.x) + 1), j1 = min(n, (int)(blockIdx.y + 1) * jchunk);
     __syncthreads();
     for (int t0 = j0; t0 < j1; t0 += kGrTile) {
         const int tn = min(kGrTile, j1 - t0);
@@ -61,16 +81,16 @@ __global__ void __launch_bounds__(256) k_gr_batch(const float4 *__restrict__ sna
             if (vi && j > i) {
                 float4 pj = tile[t];
                 float dx = __fsub_rn(pi.x, pj.x), dy = __fsub_rn(pi.y, pj.y), dz = __fsub_rn(pi.z, pj.z);
-                int bf = gr_bin(dx, dy, dz, side, side_inv, range, range2_hi, bin_size, nbins);
+                int bf = gr_bin(dx, dy, dz, side, side_inv, thr, inv_bin_size, nbins);
                 // below 0.49 the minimum image returns d itself for both signs
                 // (min_image_gder_fast), so the reverse distance is the same
                 bool sym = fabsf(__fmul_rn(side_inv, dx)) < 0.49f && fabsf(__fmul_rn(side_inv, dy)) < 0.49f &&
                            fabsf(__fmul_rn(side_inv, dz)) < 0.49f;
-                int bb = sym ? bf : gr_bin(-dx, -dy, -dz, side, side_inv, range, range2_hi, bin_size, nbins);
+                int bb = sym ? bf : gr_bin(-dx, -dy, -dz, side, side_inv, thr, inv_bin_size, nbins);
                 if (bf >= 0) kf = (ti * 2 + tj) * nbins + bf;
                 if (bb >= 0) kr = (tj * 2 + ti) * nbins + bb;
             }
-            if (per_warp) {
+            if (copies > 1) {
                 if (kf >= 0) atomicAdd(&hist[kf], 1u);
                 if (kr >= 0) atomicAdd(&hist[kr], 1u);
             } else {
@@ -1002,27 +1022,42 @@ int bd_engine_gder_method(bd_engine *e, int nbins, float range, int method, unsi
     }
     unsigned long long *d_counts = nullptr;
     const size_t per = (size_t)4 * nbins;
-    BD_CUDA_TRY(cudaMalloc(&d_counts, sizeof(unsigned long long) * per * e->R));
+    // counts, then the nbins + 2 bin thresholds (gr_bin_thr)
+    BD_CUDA_TRY(cudaMalloc(&d_counts, sizeof(unsigned long long) * per * e->R + sizeof(float) * (nbins + 2)));
+    float *d_thr = reinterpret_cast<float *>(d_counts + per * e->R);
     cudaMemsetAsync(d_counts, 0, sizeof(unsigned long long) * per * e->R, e->stream);
-    int rc = launch_gder_cells(e, m_of, nbins, range, d_counts);  // may hand replicas back
+    k_gr_thresholds<<<div_up(nbins + 2, 128), 128, 0, e->stream>>>(range, nbins, d_thr);
+    int rc = launch_gder_cells(e, m_of, nbins, range, d_thr, d_counts);  // may hand replicas back
     for (int r = 0; r < e->R; r++) any_all |= m_of[r] < 0;
     cudaError_t le = cudaSuccess;
     if (rc == BD_OK && any_all) {
         k_export<<<div_up(e->C, 128), 128, 0, e->stream>>>(e->cnt[obs_buf(e)], e->pos[obs_buf(e)], (int)e->C, e->cap, (int)e->P,
                                                            e->gid_of, e->x0, e->dsp[0], e->dsp[1], e->dsp[2], nullptr,
                                                            nullptr, e->snap);
-        // one histogram copy per warp when 8 of them fit beside the tile
-        const int per_warp = (size_t)8 * per * sizeof(unsigned) <= 160 * 1024 ? 1 : 0;
-        const size_t sm = kGrTile * sizeof(float4) + (per_warp ? 8 : 1) * per * sizeof(unsigned);
+        // one histogram copy per two warps when 4 of them fit beside the tile
+        const int copies = (size_t)4 * per * sizeof(unsigned) <= 96 * 1024 ? 4 : 1;
+        const size_t sm = kGrTile * sizeof(float4) + sizeof(float) * (nbins + 2) + copies * per * sizeof(unsigned);
         cudaFuncSetAttribute(k_gr_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         const int jchunk = 8192;
-        for (int r = 0; r < e->R; r++) {
-            if (m_of[r] >= 0) continue;
-            const SysDev &S = e->sysh[r];
-            dim3 grid(div_up(S.n, 256), div_up(S.n, jchunk));
-            k_gr_batch<<<grid, 256, sm, e->stream>>>(e->snap + S.part_base, S.n, S.n_big, S.L, range, nbins, jchunk,
-                                                     per_warp, d_counts + per * r);
+        std::vector<int> reps;
+        int nmax = 0;
+        for (int r = 0; r < e->R; r++)
+            if (m_of[r] < 0) {
+                reps.push_back(r);
+                nmax = std::max(nmax, e->sysh[r].n);
+            }
+        int *d_reps = nullptr;
+        le = cudaMalloc(&d_reps, sizeof(int) * reps.size());
+        if (le == cudaSuccess)
+            le = cudaMemcpyAsync(d_reps, reps.data(), sizeof(int) * reps.size(), cudaMemcpyHostToDevice, e->stream);
+        if (le == cudaSuccess && nmax > 0) {
+            dim3 grid(div_up(nmax, 256), div_up(nmax, jchunk), (unsigned)reps.size());
+            k_gr_batch<<<grid, 256, sm, e->stream>>>(e->snap, e->d_sys, d_reps, range, d_thr, nbins, jchunk, copies,
+                                                     d_counts);
         }
+        if (le == cudaSuccess) le = cudaStreamSynchronize(e->stream);
+        if (d_reps) cudaFree(d_reps);
+        if (le != cudaSuccess) rc = BD_ERR_CUDA;
         le = cudaGetLastError();
         if (le != cudaSuccess) rc = BD_ERR_CUDA;
     }

@@ -96,7 +96,7 @@ namespace bd {
 // wrap) and the launch over the replicas with m_of[r] >= 0; replicas it
 // cannot count come back with m_of[r] = -1
 int gder_cell_reach(const SysDev &S, float range);
-int launch_gder_cells(bd_engine *e, std::vector<int> &m_of, int nbins, float range,
+int launch_gder_cells(bd_engine *e, std::vector<int> &m_of, int nbins, float range, const float *d_thr,
                       unsigned long long *d_counts);
 
 // cell-bucket buffer holding the current state (list mode rebuilds buffer 0

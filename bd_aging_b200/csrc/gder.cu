@@ -46,6 +46,7 @@ struct GrArgs {
     int cap;
     int nbins;
     float range;
+    const float *thr;            // [nbins + 2] bin thresholds (gr_bin_thr)
     unsigned long long *counts;  // [R][4][nbins]
     const int *m_of;             // stencil reach in cells, per replica
     int *misplaced;              // per replica: a particle lies outside its cell
@@ -96,24 +97,19 @@ __device__ int gr_scan(int *a, int n, int *wsum) {
 
 // last index c in [0, n) with start[c] <= t
 // one unordered pair (i, j) within range: both ordered counts
-__device__ __forceinline__ void gr_count_pair(float4 pi, float4 pj, float side, float side_inv, float range,
-                                              float range2_hi, float bin_size, int nbins, unsigned *hist) {
+__device__ __forceinline__ void gr_count_pair(float4 pi, float4 pj, float side, float side_inv, const float *thr,
+                                              float inv_bin_size, int nbins, unsigned *hist) {
     const float dx = min_image_gder_fast(__fsub_rn(pi.x, pj.x), side, side_inv);
     const float dy = min_image_gder_fast(__fsub_rn(pi.y, pj.y), side, side_inv);
     const float dz = min_image_gder_fast(__fsub_rn(pi.z, pj.z), side, side_inv);
-    const float d2 = dist2_rn(dx, dy, dz);
-    if (d2 <= range2_hi) {
-        const float dist = __fsqrt_rn(d2);
-        if (dist < range) {
-            int bin = (int)__fdiv_rn(dist, bin_size);
-            if (bin == nbins) bin--;
-            const unsigned ti = __float_as_uint(pi.w) >> 31, tj = __float_as_uint(pj.w) >> 31;
-            if (ti == tj) {
-                atomicAdd(&hist[3 * ti * nbins + bin], 2u);
-            } else {
-                atomicAdd(&hist[(2 * ti + tj) * nbins + bin], 1u);
-                atomicAdd(&hist[(2 * tj + ti) * nbins + bin], 1u);
-            }
+    const int bin = gr_bin_thr(dist2_rn(dx, dy, dz), thr, inv_bin_size, nbins);
+    if (bin >= 0) {
+        const unsigned ti = __float_as_uint(pi.w) >> 31, tj = __float_as_uint(pj.w) >> 31;
+        if (ti == tj) {
+            atomicAdd(&hist[3 * ti * nbins + bin], 2u);
+        } else {
+            atomicAdd(&hist[(2 * ti + tj) * nbins + bin], 1u);
+            atomicAdd(&hist[(2 * tj + ti) * nbins + bin], 1u);
         }
     }
 }
@@ -135,6 +131,7 @@ __global__ void __launch_bounds__(kGrThreads) k_gr_cells(GrArgs a) {
     int *cgc = cstart + kGrTileCells + 1;                       // [kGrTileCells]
     int *wsum = cgc + kGrTileCells;                             // [kGrThreads / 32 + 1]
     unsigned *hist = reinterpret_cast<unsigned *>(wsum + kGrThreads / 32 + 4);  // [4][nbins]
+    float *thr = reinterpret_cast<float *>(hist + 4 * a.nbins);                   // [nbins + 2]
     const int tid = threadIdx.x;
     const int4 br = a.bricks[blockIdx.x];
     const SysDev &S = a.sys[br.x];
@@ -145,8 +142,7 @@ __global__ void __launch_bounds__(kGrThreads) k_gr_cells(GrArgs a) {
     const float side = S.L;
     const float side_inv = __double2float_rn(1.0 / (double)side);
     const float range = a.range;
-    const float bin_size = __fdiv_rn(range, (float)nbins);
-    const float range2_hi = range * range * 1.00001f;
+    const float inv_bin_size = 1.0f / __fdiv_rn(range, (float)nbins);  // estimate only (gr_bin_thr)
     // cells whose nearest point is farther than range: gap g (cells) with
     // g cs - 4 tol > range (cell units, with margin)
     const float cs = side / (float)nc;
@@ -154,6 +150,7 @@ __global__ void __launch_bounds__(kGrThreads) k_gr_cells(GrArgs a) {
     const float lim = (range / cs) * 1.00001f + 4.0f * (float)kGrTol;
     const float lim2 = lim * lim;
     for (int b = tid; b < 4 * nbins; b += kGrThreads) hist[b] = 0;
+    for (int b = tid; b < nbins + 2; b += kGrThreads) thr[b] = a.thr[b];
 
     // 1. home particles of the brick
     const int nhc = wx * wy * wz;
@@ -193,7 +190,7 @@ __global__ void __launch_bounds__(kGrThreads) k_gr_cells(GrArgs a) {
             for (int p = tid; p < nhh; p += kGrThreads) {
                 const float4 pi = home[h], pj = home[c];
                 if ((__float_as_uint(pi.w) & 0x7fffffffu) < (__float_as_uint(pj.w) & 0x7fffffffu))
-                    gr_count_pair(pi, pj, side, side_inv, range, range2_hi, bin_size, nbins, hist);
+                    gr_count_pair(pi, pj, side, side_inv, thr, inv_bin_size, nbins, hist);
                 h += dh;
                 c += dc;
                 if (h >= H) { h -= H; c++; }
@@ -241,7 +238,7 @@ __global__ void __launch_bounds__(kGrThreads) k_gr_cells(GrArgs a) {
             const int np = H * Tn;
             int h = tid % H, c = tid / H;
             for (int p = tid; p < np; p += kGrThreads) {
-                gr_count_pair(home[h], tile[c], side, side_inv, range, range2_hi, bin_size, nbins, hist);
+                gr_count_pair(home[h], tile[c], side, side_inv, thr, inv_bin_size, nbins, hist);
                 h += dh;
                 c += dc;
                 if (h >= H) { h -= H; c++; }
@@ -268,13 +265,13 @@ int gder_cell_reach(const SysDev &S, float range) {
 
 size_t gder_cells_smem(int nbins) {
     return sizeof(float4) * (kGrHomeMax + kGrTileMax) + sizeof(int) * (2 * kGrTileCells + 1 + kGrThreads / 32 + 4) +
-           sizeof(unsigned) * 4 * (size_t)nbins;
+           sizeof(unsigned) * 4 * (size_t)nbins + sizeof(float) * (nbins + 2);
 }
 
 // Counts of the replicas with m_of[r] >= 0 into d_counts.  A replica whose
 // particles are not all inside their cells gets m_of[r] = -1 and zero counts
 // (the caller recounts it with all pairs).
-int launch_gder_cells(bd_engine *e, std::vector<int> &m_of, int nbins, float range,
+int launch_gder_cells(bd_engine *e, std::vector<int> &m_of, int nbins, float range, const float *d_thr,
                       unsigned long long *d_counts) {
     std::vector<int4> bricks;
     for (int r = 0; r < e->R; r++) {
@@ -309,6 +306,7 @@ int launch_gder_cells(bd_engine *e, std::vector<int> &m_of, int nbins, float ran
         a.cap = e->cap;
         a.nbins = nbins;
         a.range = range;
+        a.thr = d_thr;
         a.counts = d_counts;
         a.m_of = d_m;
         a.misplaced = d_bad;

@@ -72,3 +72,29 @@ def test_cells_equal_all_pairs_at_quarter_million():
     np.testing.assert_array_equal(a, b)
     # every particle sees its own neighbourhood: bs and sb counts match
     np.testing.assert_array_equal(a[0, 1].sum(), a[0, 2].sum())
+
+
+@pytest.mark.parametrize("method", ["cells", "all_pairs"])
+def test_bin_edges_on_a_lattice_match_oracle(method):
+    # A simple cubic lattice of spacing 0.5 (every coordinate exact in float):
+    # distances 0.5 sqrt(n) put many pairs exactly on edges of the 0.01-wide
+    # bins (n a perfect square) and the rest anywhere, so the bin rounding of
+    # the reference (sqrt, then divide, both correctly rounded) is checked
+    # where a one-ulp slip would move a count to the next bin.
+    k = 24
+    side = 0.5 * k
+    g = (np.arange(k, dtype=np.float32) * np.float32(0.5)) + np.float32(0.25)
+    pos = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3).astype(np.float32)
+    nb = len(pos) // 2
+    s = B.System(n_big=nb, n_sml=len(pos) - nb, side=side, sigma_big=0.3, sigma_sml=0.2, dt=1e-6, seed=1,
+                 T0=0.0, protocol="const")
+    e = B.Engine([s], neighbor_skin=0.0)
+    e.set_positions(pos)
+    nbins, range_ = 300, 3.0
+    got = e.gder(nbins, range_, method=method)[0]
+    snap, _ = e.get_positions()
+    np.testing.assert_array_equal(snap, pos)
+    p = O.setup_params(side, s.n_big, s.n_sml, 0.3, 0.2, nbins=nbins, rng=range_)
+    ref = O.gder_counts(p, snap[: s.n_big], snap[s.n_big:])
+    np.testing.assert_array_equal(got, ref)
+    assert got.sum() > 0
