@@ -276,6 +276,7 @@ ListArgs make_largs(bd_engine *e, int cur) {
     a.nbr = e->nbr;
     a.nnb = e->nnb;
     a.pbuild = e->pbuild;
+    a.amp_tab = e->amp_tab;
     a.flag = e->lflag;
     a.nrep = e->R;
     a.x0 = e->x0;
@@ -367,9 +368,19 @@ int sync_buckets(bd_engine *e) {
     return rc ? rc : list_bin(e, e->cur, e->d_one, nullptr);
 }
 
+// noise amplitudes of the next `count` list steps (count <= graph_steps)
+int list_amplitudes(bd_engine *e, int count) {
+    const int n = count * e->R;
+    k_amp_table<<<div_up(n, 256), 256, 0, e->stream>>>(e->d_sys, e->R, e->d_ni, e->ni_first, count, e->amp_tab);
+    BD_LAUNCH_CHECK();
+    return BD_OK;
+}
+
 // k steps outside graphs (k = 1 in plain mode): launch, advance the counter
 int direct_steps(bd_engine *e, int k) {
     if (e->list) {
+        if (k > e->graph_steps) return BD_ERR_ARG;  // the amplitude table holds one batch
+        if (int rc = list_amplitudes(e, k)) return rc;
         for (int i = 0; i < k; i++) {
             int rc = list_step(e, e->cur + i, i);
             if (rc) return rc;
@@ -398,6 +409,7 @@ int build_graph(bd_engine *e) {
     BD_CUDA_TRY(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
     int rc = BD_OK;
     if (e->list) {
+        rc = list_amplitudes(e, e->graph_steps);
         for (int j = 0; j < e->graph_steps && rc == BD_OK; j++) rc = list_step(e, e->cur + j, j);
     } else if (e->mode == BD_MODE_PERSISTENT) {
         StepArgs a = make_args(e, e->cur, 1);
@@ -426,7 +438,7 @@ void free_engine(bd_engine *e) {
                     e->status, e->d_ni, e->out_pos, e->out_raw, e->d_cl_start, e->d_cl_bricks, e->rn_ring, e->rn_lcg,
                     e->snaps, e->d_segs, e->d_seg_first, e->corr_part, e->corr_out, e->lpos[0], e->lpos[1],
                     e->pbuild, e->nbr, e->nnb, e->lflag, e->d_one, e->d_builds, e->ld_in, e->ld_staged,
-                    e->ld_slot, e->ld_bucket, e->ld_cnt, e->ld_start, e->ld_bsum, e->ld_bad, e->img};
+                    e->ld_slot, e->ld_bucket, e->ld_cnt, e->ld_start, e->ld_bsum, e->ld_bad, e->img, e->amp_tab};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -689,6 +701,7 @@ int bd_engine_create(const bd_system_desc *systems, int nsys, const bd_engine_op
         ALLOC(e->nbr, sizeof(int) * (size_t)kMaxNbr * P);
         ALLOC(e->nnb, sizeof(int) * P);
         ALLOC(e->img, sizeof(int) * 3 * P);
+        ALLOC(e->amp_tab, sizeof(float) * 2 * (size_t)e->R * e->graph_steps);
         ALLOC(e->lflag, sizeof(int) * (e->R + 1));
         ALLOC(e->d_one, sizeof(int));
         ALLOC(e->d_builds, 2 * sizeof(long long));

@@ -49,6 +49,7 @@ struct ListArgs {
     int *img;               // [3][np]: box lengths crossed per axis since the origin
     const int *nbr;         // [kMaxNbr][np]
     const int *nnb;         // [np]
+    const float *amp_tab;   // [step in launch batch][R][species] noise amplitudes (k_amp_table)
     const float4 *pbuild;   // positions at the last build
     int *flag;              // [R + 1]: flag[r] replica r needs a rebuild, flag[R] any does
     int nrep;
@@ -420,7 +421,8 @@ __global__ void __launch_bounds__(BD_LIST_THREADS, BD_LIST_MINB) k_step_list(Lis
     const int sid = blockIdx.x * blockDim.x + threadIdx.x;
     if (sid >= a.np) return;
     const long long ni = *ni_base + ni_off;
-    const SysDev &S = a.sys[a.rep_of_sid[sid]];
+    const int rep = a.rep_of_sid[sid];
+    const SysDev &S = a.sys[rep];
     const float L = S.L, Linv = S.Linv;
     const float4 pi = a.pos_in[sid];
     const unsigned wi = __float_as_uint(pi.w);
@@ -482,7 +484,7 @@ __global__ void __launch_bounds__(BD_LIST_THREADS, BD_LIST_MINB) k_step_list(Lis
         xi = make_float3(a.noise[3 * (size_t)gid], a.noise[3 * (size_t)gid + 1], a.noise[3 * (size_t)gid + 2]);
     }
     const float mob = S.mob[tm], dt = S.dt;
-    const float amp = amplitude(step_temperature(S, ni, a.ni_first), mob, dt);
+    const float amp = a.amp_tab[((size_t)ni_off * a.nrep + rep) * 2 + tm];
     const float ex = __fadd_rn(__fmul_rn(__fmul_rn(fx, mob), dt), __fmul_rn(amp, xi.x));
     const float ey = __fadd_rn(__fmul_rn(__fmul_rn(fy, mob), dt), __fmul_rn(amp, xi.y));
     const float ez = __fadd_rn(__fmul_rn(__fmul_rn(fz, mob), dt), __fmul_rn(amp, xi.z));
@@ -527,6 +529,21 @@ __global__ void k_list_dsp(const float4 *__restrict__ pos, const float *__restri
     dx[sid] = (((double)v.x + (double)lo_x[sid]) + L * (double)img[sid]) - x0[g];
     dy[sid] = (((double)v.y + (double)lo_y[sid]) + L * (double)img[np + sid]) - x0[g + 1];
     dz[sid] = (((double)v.z + (double)lo_z[sid]) + L * (double)img[2 * (size_t)np + sid]) - x0[g + 2];
+}
+
+// Noise amplitude of every replica and species for `count` consecutive steps
+// from *ni_base (the same temperature and amplitude arithmetic as the
+// sweep's update), once per launch batch instead of once per particle:
+// tab[(j * nrep + r) * 2 + species].
+__global__ void k_amp_table(const SysDev *sys, int nrep, const long long *ni_base, long long ni_first, int count,
+                            float *tab) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count * nrep) return;
+    const int j = t / nrep, r = t % nrep;
+    const SysDev &S = sys[r];
+    const float T = step_temperature(S, *ni_base + j, ni_first);
+    tab[2 * (size_t)t] = amplitude(T, S.mob[0], S.dt);
+    tab[2 * (size_t)t + 1] = amplitude(T, S.mob[1], S.dt);
 }
 
 // Census from the lists: interacting partners per particle and a hash of
