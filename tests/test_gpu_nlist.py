@@ -248,3 +248,29 @@ def test_many_replicas_rebuild_only_the_flagged_ones():
         _, _, _, nbr, h = O.eng_forces(pb[sl], types_of(s), s.side, SB, SS)
         np.testing.assert_array_equal(cnt[sl], nbr)
         np.testing.assert_array_equal(hsh[sl], h)
+
+
+def test_more_replicas_than_the_rebuild_scheduler_takes():
+    # above 1024 replicas the rebuild kernels walk every particle, cell and
+    # brick instead of numbering the flagged ones; the lists must be the same
+    nrep = 1030
+    temps = [2.0 if k % 5 == 0 else 1e-3 for k in range(nrep)]
+    systems, poss = zip(*[system(80, 80, 0.3, 500 + k, T0=t, protocol="const", dt=2e-4)
+                          for k, t in enumerate(temps)])
+    eb = B.Engine(list(systems), neighbor_skin=SKIN)
+    eb.set_positions(np.concatenate(poss))
+    eb.run(60)
+    pb, _ = eb.get_positions()
+    assert eb.info().list_builds > nrep + 20
+    cnt, hsh = eb.census()
+    for k in list(range(0, nrep, 97)) + [nrep - 1]:
+        s = systems[k]
+        sl = slice(eb.offsets[k], eb.offsets[k + 1])
+        _, _, _, nbr, h = O.eng_forces(pb[sl], types_of(s), s.side, SB, SS)
+        np.testing.assert_array_equal(cnt[sl], nbr)
+        np.testing.assert_array_equal(hsh[sl], h)
+    for k in (0, 1, nrep - 1):
+        e1 = B.Engine([systems[k]], neighbor_skin=SKIN)
+        e1.set_positions(poss[k])
+        e1.run(60)
+        np.testing.assert_array_equal(e1.get_positions()[0], pb[eb.offsets[k]:eb.offsets[k + 1]])
