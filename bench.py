@@ -465,9 +465,11 @@ def run_ours(args):
     tpp = profile_traffic_per_particle_step(list_mode)
     # kernels per time step: the list step plus its four rebuild kernels (which
     # exit at once when no list is stale), or the one sweep kernel; per
-    # 96-step graph the counter kernel (persistent mode: one launch per graph)
+    # 96-step graph the counter kernel, plus the noise-amplitude table in list
+    # mode (persistent mode: the persistent kernel and the counter)
     per_step = 5 if list_mode else (1 if args.mode == "plain" else 0)
-    gpu_launches = args.steps * (math.ceil(S / 96) * (1 if per_step else 2) + per_step * S)
+    per_graph = 2 if (list_mode or not per_step) else 1
+    gpu_launches = args.steps * (math.ceil(S / 96) * per_graph + per_step * S)
     line = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 forces, f32+compensation positions, f64 displacement",
