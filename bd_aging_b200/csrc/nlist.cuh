@@ -29,10 +29,10 @@ constexpr int kMaxNbr = 64;
 #define BD_LIST_GATHER 4  // list partners whose positions are in flight together
 #endif
 #ifndef BD_LIST_THREADS
-#define BD_LIST_THREADS 256  // CTA size of the list step
+#define BD_LIST_THREADS 128  // CTA size of the list step
 #endif
 #ifndef BD_LIST_MINB
-#define BD_LIST_MINB 4       // resident CTAs per SM asked of the register allocator (64 registers)
+#define BD_LIST_MINB 8       // resident CTAs per SM asked of the register allocator (64 registers)
 #endif
 constexpr int kGather = BD_LIST_GATHER;
 constexpr int kListBuildThreads = 256;  // CTA size of the list build
