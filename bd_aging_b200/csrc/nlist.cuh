@@ -14,12 +14,15 @@
 // decision.  (Conditional graph nodes around the rebuild kernels, switched on
 // by the step kernel, measured 2% slower than these four early exits.)
 //
-// State by storage id: pos[2][P] float4 (double-buffered: x, y, z and
-// w = storage id | species << 31), positions at the last build, the lists
-// [kMaxNbr][P] (slot-major: the threads of a warp read consecutive words),
-// list lengths, plus the compensated remainder and FP64 displacement shared
-// with the sweep path.  Cell buckets (cnt / pos of buffer 0) are rebuilt
-// from the by-id positions for list builds and observation passes.
+// State by storage id: pos[2][P + 1] float4 (double-buffered: x, y, z and
+// w = storage id | species << 31; entry P is the zero position that list
+// padding gathers), positions at the last build, the lists [kMaxNbr][P]
+// (slot-major: the threads of a warp read consecutive words, padded to whole
+// gather chunks), list lengths, the compensated remainder shared with the
+// sweep path, and face crossings per axis [3][P] in place of a per-step FP64
+// displacement (k_list_dsp rebuilds it for observations).  Cell buckets
+// (cnt / pos of buffer 0) are rebuilt from the by-id positions for list
+// builds and observation passes.
 #pragma once
 
 namespace bd {
