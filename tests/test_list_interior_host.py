@@ -6,8 +6,10 @@ skin + 0.01 from every face skips the minimum image.  A list partner was
 within cut + skin at the build, and each end has moved at most skin/2 since,
 so the partner's stored (wrapped) coordinate lies in the same image.  The
 plain float difference is then what the reference's minimum image
-(get_forces.cu:389-391, float) returns.  Checked on random particles, partners
-and boxes, including partners placed at the largest allowed distance."""
+(get_forces.cu:389-391, float) returns, and the zero position that list
+padding gathers lies beyond every cut distance.  Checked on random particles,
+partners and boxes, including partners placed at the largest allowed
+distance."""
 import numpy as np
 import pytest
 
@@ -42,3 +44,8 @@ def test_interior_partners_need_no_minimum_image(L, rcmax, skin):
     np.testing.assert_array_equal(min_image_ref(d, L, Linv), d)
     # and the plain difference is the true one (no wrap happened)
     np.testing.assert_allclose(d, (pj_true - pi).astype(F), atol=1e-5)
+    # padding entries gather the zero position: from an interior particle it
+    # is farther than every cut distance, so they need no index test there
+    d0 = (F(0) - pi).astype(F)
+    d2 = ((d0[:, 0] * d0[:, 0]).astype(F) + (d0[:, 1] * d0[:, 1]).astype(F)).astype(F) + (d0[:, 2] * d0[:, 2]).astype(F)
+    assert np.all(d2.astype(F) >= F(rcmax) ** 2)
