@@ -2,6 +2,7 @@
 // kernels behind the C ABI of include/bd_aging.h.  Same argument meaning and
 // float3 array-of-structs layout as the reference; status codes instead of
 // exit(); explicit streams; no write ever leaves its buffer.
+#include <cuda.h>
 #include <curand_kernel.h>
 
 #include <cmath>
@@ -14,17 +15,49 @@
 namespace bd {
 
 // ------------------------------------------------------------ workspace
+unsigned long long current_context_id() {
+    using GetCurrent = CUresult (*)(CUcontext *);
+    using GetId = CUresult (*)(CUcontext, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = (GetCurrent)f;
+        f = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (GetId)f;
+    });
+    if (!get_current || !get_id) return 0;
+    CUcontext c = nullptr;
+    if (get_current(&c) != CUDA_SUCCESS || !c) {
+        int dev = 0;  // no context yet on this thread: make the device's primary context current
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaSetDevice(dev) != cudaSuccess) return 0;
+        if (get_current(&c) != CUDA_SUCCESS || !c) return 0;
+    }
+    unsigned long long id = 0;
+    return get_id(c, &id) == CUDA_SUCCESS ? id + 1 : 0;  // +1: a valid id is never 0 here
+}
+
 DeviceWork *device_work() {
     static std::mutex mu;
     static DeviceWork works[64];
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    const unsigned long long ctx = current_context_id();
+    if (!ctx) return nullptr;
     std::lock_guard<std::mutex> lock(mu);
     DeviceWork &w = works[dev];
-    if (!w.status) {
+    if (w.ctx != ctx) {  // first use, or the context was destroyed (its memory with it)
+        w = DeviceWork{};
         if (cudaMalloc(&w.status, 256) != cudaSuccess) return nullptr;
-        if (cudaMalloc(&w.accum, 16 * sizeof(double)) != cudaSuccess) return nullptr;
-        cudaMemset(w.status, 0, 256);
+        if (cudaMalloc(&w.accum, kWorkAccum * sizeof(double)) != cudaSuccess) return nullptr;
+        if (cudaMemset(w.status, 0, 256) != cudaSuccess) return nullptr;
+        w.ctx = ctx;
     }
     return &w;
 }
@@ -257,9 +290,14 @@ __global__ void __launch_bounds__(256) k_gder(const float *__restrict__ ra, int 
 // ------------------------------------------------------------ F_s, MSD
 // fself_isotropic (fself.cu:3-21) and the MSD loop (main.cu:776-792): per
 // particle float terms as in the reference, summed in FP64.
+// One FP64 partial per block, then one block adds the partials in index
+// order, so the result does not depend on the order in which blocks finish.
+constexpr int kDispThreads = 256, kDispMaxBlocks = 148 * 8;
+static_assert(kDispMaxBlocks + 1 <= kWorkAccum, "partials fit the workspace");
 template <int KIND>  // 0: F_s, 1: MSD
-__global__ void k_disp_reduce(const float *__restrict__ raw, const float *__restrict__ r0, int n, float q,
-                              double *acc) {
+__global__ void __launch_bounds__(kDispThreads) k_disp_reduce(const float *__restrict__ raw,
+                                                              const float *__restrict__ r0, int n, float q,
+                                                              double *part) {
     double s = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float dx = raw[3 * i] - r0[3 * i], dy = raw[3 * i + 1] - r0[3 * i + 1], dz = raw[3 * i + 2] - r0[3 * i + 2];
@@ -272,23 +310,37 @@ __global__ void k_disp_reduce(const float *__restrict__ raw, const float *__rest
         }
     }
     for (int o = 16; o; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    __shared__ double red[32];
+    __shared__ double red[kDispThreads / 32];
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
     __syncthreads();
-    if (threadIdx.x < 32) {
-        s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
-        for (int o = 16; o; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-        if (threadIdx.x == 0) atomicAdd(acc, s);
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kDispThreads / 32; w++) t += red[w];
+        part[1 + blockIdx.x] = t;
     }
+}
+// part[0] = sum of part[1 .. nblocks] in a fixed order
+__global__ void __launch_bounds__(kDispThreads) k_disp_finish(double *part, int nblocks) {
+    __shared__ double red[kDispThreads];
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += part[1 + b];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = kDispThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[0] = red[0];
 }
 
 static int disp_reduce(int kind, const float *raw, const float *r0, int n, float q, double *out, cudaStream_t s) {
     DeviceWork *w = device_work();
     if (!w) return BD_ERR_NOMEM;
-    BD_CUDA_TRY(cudaMemsetAsync(w->accum, 0, sizeof(double), s));
-    int blocks = std::min(div_up(n, 256), 148 * 8);
-    if (kind == 0) k_disp_reduce<0><<<blocks, 256, 0, s>>>(raw, r0, n, q, w->accum);
-    else k_disp_reduce<1><<<blocks, 256, 0, s>>>(raw, r0, n, q, w->accum);
+    const int blocks = std::min(div_up(n, kDispThreads), kDispMaxBlocks);
+    if (kind == 0) k_disp_reduce<0><<<blocks, kDispThreads, 0, s>>>(raw, r0, n, q, w->accum);
+    else k_disp_reduce<1><<<blocks, kDispThreads, 0, s>>>(raw, r0, n, q, w->accum);
+    BD_LAUNCH_CHECK();
+    k_disp_finish<<<1, kDispThreads, 0, s>>>(w->accum, blocks);
     BD_LAUNCH_CHECK();
     BD_CUDA_TRY(cudaMemcpyAsync(out, w->accum, sizeof(double), cudaMemcpyDeviceToHost, s));
     BD_CUDA_TRY(cudaStreamSynchronize(s));

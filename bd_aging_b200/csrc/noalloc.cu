@@ -1,11 +1,11 @@
 // noalloc.cu -- F_s(q) reduction that allocates nothing on the device.
 //
-// bd_fself_isotropic (mirror.cu) keeps its FP64 accumulator in a per-device
+// bd_fself_isotropic (mirror.cu) keeps its FP64 partial sums in a per-device
 // workspace that is cudaMalloc'd on first use.  Some callers cannot allocate
-// device memory at the moment they sample F_s: code that runs while a CUDA
-// stream is being captured in global capture mode (where cudaMalloc is an
-// illegal call), real-time sampling loops that forbid allocation, or hosts
-// whose device memory is fully reserved by another allocator.  For them,
+// device memory at the moment they sample F_s: real-time sampling loops whose
+// rules forbid allocation after start-up, and host programs whose device
+// memory is fully reserved up front by another allocator (a pool that owns
+// the GPU), where a late cudaMalloc fails or fragments the pool.  For them,
 // bd_fself_isotropic_noalloc does the same reduction with its scratch in the
 // fixed array below.
 //
@@ -14,13 +14,15 @@
 // particles, so ngrain is limited to kFselfScratchBlocks * 256 = 1,048,576;
 // larger calls are rejected with BD_ERR_ARG before any work is queued.
 // The partial sums are overwritten by every call (nothing accumulates into
-// the array, so nothing needs clearing); calls that overlap on the GPU (two
-// streams, or two host threads) race on the array.
+// the array, so nothing needs clearing).  All calls on a GPU share the one
+// array: calls that overlap on the GPU (two streams, or two host threads)
+// race on it, so callers must serialise them.
 //
 // Set-up: host code cannot use the array's name as a device address, so the
-// first call on each device looks the address up with cudaGetSymbolAddress
-// (with that device current) and caches it.  Make that first call on a
-// device before any stream capture begins.
+// first call on each device (with that device current) looks the address up
+// with cudaGetSymbolAddress and caches it for that device's context; a device
+// reset, which destroys the context, makes the next call look it up again.
+// Make that first call on a device before any stream capture begins.
 #include <mutex>
 
 #include "runtime.cuh"
@@ -70,17 +72,23 @@ __global__ void k_fself_finish(double *part, int nblocks) {
     if (threadIdx.x == 0) part[0] = red[0];
 }
 
-// device address of g_fself_scratch, looked up once per device
+// device address of g_fself_scratch, looked up once per device and context
 static double *fself_scratch_address(int *rc) {
     static std::mutex mu;
     static double *addr[64] = {nullptr};
+    static unsigned long long ctx_of[64] = {0};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
         *rc = BD_ERR_CUDA;
         return nullptr;
     }
+    const unsigned long long ctx = current_context_id();
+    if (!ctx) {
+        *rc = BD_ERR_CUDA;
+        return nullptr;
+    }
     std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev]) {
+    if (!addr[dev] || ctx_of[dev] != ctx) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_fself_scratch);
         if (e != cudaSuccess || !p) {
@@ -88,6 +96,7 @@ static double *fself_scratch_address(int *rc) {
             return nullptr;
         }
         addr[dev] = (double *)p;
+        ctx_of[dev] = ctx;
     }
     *rc = BD_OK;
     return addr[dev];

@@ -13,12 +13,20 @@ namespace bd {
 
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
-// Small per-device workspace for the mirror entry points: a status word and
-// a few FP64 accumulators.  Allocated once per device on first use and kept
-// until process exit.
+// Identifier of the CUDA context current on the calling thread (initialising
+// the current device's primary context if needed).  Context ids are unique
+// for the life of the process, so a device reset, which destroys the primary
+// context and every address in it, changes the id.  0 when none can be had.
+unsigned long long current_context_id();
+
+// Per-device workspace for the mirror entry points: a status word and the
+// FP64 partial sums of the fixed-order reductions.  Allocated on first use in
+// each device's context (again after a device reset) and kept until exit.
+constexpr int kWorkAccum = 2048;  // FP64 slots: one per reduction block plus the result
 struct DeviceWork {
     unsigned *status = nullptr;   // device status word (kStat* bits)
-    double *accum = nullptr;      // 16 FP64 accumulators
+    double *accum = nullptr;      // kWorkAccum FP64 partial sums
+    unsigned long long ctx = 0;   // context the pointers belong to
 };
 
 DeviceWork *device_work();  // nullptr on allocation failure

@@ -158,24 +158,25 @@ int bd_gder_normalize(const double *counts, int nbins, float bin_size, float sid
                       int ngrain_sml, float sigma_big, float sigma_sml, int n_configs, float *gder);
 
 /* fself_isotropic (fself.cu:3-21): adds (1/N) sum sin(q|dr|)/(q|dr|) over
- * dr = rr_raw - rr0 to fself_host[sample_number].  Device inputs, host
+ * dr = rr_raw - rr0 to fself_host[sample_number].  The FP64 sum runs in a
+ * fixed order, so repeated calls give identical bits.  Device inputs, host
  * output, stream-synchronous. */
 int bd_fself_isotropic(const float *rr_raw, const float *rr0, int ngrain, float *fself_host, int sample_number,
                        float qmax, void *stream);
 
 /* No counterpart in the reference.  Same result as bd_fself_isotropic for
- * callers that cannot allocate device memory when they sample F_s (inside a
- * stream capture in global capture mode, real-time loops, hosts whose device
- * memory is reserved by another allocator): its scratch is a fixed 32 KB
- * device array per GPU, held until process exit, so it calls no cudaMalloc.
- * Limit: ngrain <= 1,048,576, larger calls return BD_ERR_ARG.  The first call
- * on a device looks up the scratch address; make it before any stream
- * capture.  Calls that overlap on the GPU share the scratch and race. */
+ * callers that cannot allocate device memory when they sample F_s: real-time
+ * loops that forbid allocation after start-up, and programs whose device
+ * memory is reserved up front by another allocator.  Its scratch is a fixed
+ * 32 KB device array per GPU, held until process exit, so it calls no
+ * cudaMalloc.  Limit: ngrain <= 1,048,576, larger calls return BD_ERR_ARG.
+ * The first call on a device looks up the scratch address; make it before
+ * any stream capture.  All calls on a GPU share the scratch: calls that
+ * overlap on the GPU (two streams or threads) race, so serialise them.
+ * Device inputs, host output, stream-synchronous. */
 int bd_fself_isotropic_noalloc(const float *rr_raw, const float *rr0, int ngrain, float *fself_host,
                                int sample_number, float qmax, void *stream);
 
-/* Mean squared displacement of main.cu:776-792 for one species: returns
- * (1/N) sum |rr_raw - rr0|^2 in *msd_host.  Stream-synchronous. */
 /* calculate_color (colors.cu:64-110) for every big particle, as the snapshot
  * pass of main.cu:663-713 does (compiled in with GRO_FLAG): colour ids
  * (device, ngrain_big ints, or NULL) 0 blue (no big neighbour), 1 green,
@@ -183,6 +184,9 @@ int bd_fself_isotropic_noalloc(const float *rr_raw, const float *rr0, int ngrain
  * without); counts_host[3] = blue, green, red (color_statistics.out). */
 int bd_color_statistics(const float *rr_big, const float *rr_sml, int *color_ids, int *counts_host,
                         const bd_parametros *p, void *stream);
+
+/* Mean squared displacement of main.cu:776-792 for one species: returns
+ * (1/N) sum |rr_raw - rr0|^2 in *msd_host.  Stream-synchronous. */
 int bd_msd(const float *rr_raw, const float *rr0, int ngrain, float *msd_host, void *stream);
 
 /* ---- Contracting_Vector3D (Contracting_Vector3D.cuh:39-75) --------------- */
