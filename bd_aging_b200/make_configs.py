@@ -21,6 +21,24 @@ from . import configs as CF
 from . import lib as B
 
 
+def relaxed_batch(systems, seed, steps=2000, force_cap=100.0, dt_relax=1e-4):
+    """Start states of a batch of replicas: uniform random positions (replica
+    k drawn with seed + k) relaxed together by `steps` capped-force steps
+    (|F| <= force_cap, dt_relax, T = 1, Philox stream 1) on the GPU, or, with
+    steps <= 0, jittered lattices.  Returns positions [sum N, 3]."""
+    if steps <= 0:
+        return np.concatenate([CF.lattice_config(s.n_big, s.n_sml, s.side, seed + k, jitter=0.05)
+                               for k, s in enumerate(systems)])
+    pos = np.concatenate([CF.uniform_config(s.n_big, s.n_sml, s.side, seed + k) for k, s in enumerate(systems)])
+    relax = [dataclasses.replace(s, dt=dt_relax, protocol="const", T0=1.0, force_cap=force_cap) for s in systems]
+    e = B.Engine(relax, rng_stream=1)
+    e.set_positions(pos)
+    e.run(steps)
+    p, _ = e.get_positions()
+    e.close()
+    return p
+
+
 def make(n_big, n_sml, phi, n_configs, seed=1, relax_steps=2000, equil_steps=0, temp=1.0, force_cap=100.0,
          dt_relax=1e-4, dt_equil=1e-5, mobility="reference"):
     """Returns (side, positions [n_configs, N, 3])."""

@@ -108,20 +108,8 @@ def workload_systems(name, replicas, rank):
 def relaxed_positions(systems, seed, steps=2000):
     """Uniform random positions relaxed by `steps` capped-force steps on the
     GPU (Philox stream 1), all replicas at once; steps=0: jittered lattice."""
-    from bd_aging_b200 import configs as CF
-    from bd_aging_b200 import lib as B
-    import dataclasses
-    if steps <= 0:
-        return np.concatenate([CF.lattice_config(s.n_big, s.n_sml, s.side, seed + k, jitter=0.05)
-                               for k, s in enumerate(systems)])
-    pos = np.concatenate([CF.uniform_config(s.n_big, s.n_sml, s.side, seed + k) for k, s in enumerate(systems)])
-    relax = [dataclasses.replace(s, dt=1e-4, protocol="const", T0=1.0, force_cap=100.0) for s in systems]
-    e = B.Engine(relax, rng_stream=1)
-    e.set_positions(pos)
-    e.run(steps)
-    p, _ = e.get_positions()
-    e.close()
-    return p
+    from bd_aging_b200 import make_configs as MC
+    return MC.relaxed_batch(systems, seed, steps)
 
 
 # ------------------------------------------------------------------ clocks

@@ -483,6 +483,31 @@ void or_eng_forces(int n, const float *pos, const int *type, float side, const f
     }
 }
 
+/* Force cap of the initial relaxation (the reference ships no generator,
+ * run-fself.sh:84-86; the engine relaxes random placements with capped
+ * forces): a force whose magnitude exceeds fcap is scaled to magnitude fcap
+ * along its direction, computed as g = F / max|F_k|, |g|, F' = g * (fcap / |g|);
+ * a force with a non-finite component (an overlap so deep that the pair
+ * force overflows) becomes zero.  In place on ff[3n]. */
+void or_eng_cap_forces(int n, float *ff, float fcap) {
+    for (int m = 0; m < n; m++) {
+        float *f = ff + 3 * m;
+        float fmx = fmaxf(fabsf(f[0]), fmaxf(fabsf(f[1]), fabsf(f[2])));
+        if (fmx > 0.0f && isfinite(fmx)) {
+            float gx = f[0] / fmx, gy = f[1] / fmx, gz = f[2] / fmx;
+            float ng = sqrtf(gx * gx + gy * gy + gz * gz);
+            if (fmx * ng > fcap) {
+                float sc = fcap / ng;
+                f[0] = gx * sc;
+                f[1] = gy * sc;
+                f[2] = gz * sc;
+            }
+        } else if (!isfinite(fmx)) {
+            f[0] = f[1] = f[2] = 0.0f;
+        }
+    }
+}
+
 /* amplitude of the random displacement, update_ermak.cu:114 with the
  * mobility mob in place of 1/sigma: (float) sqrt(2.0 * T * mob * dt). */
 float or_eng_amplitude(float temp, float mob, float dt) { return (float)sqrt(2.0 * temp * mob * dt); }

@@ -77,6 +77,7 @@ void or_eng_forces(int n, const float *pos, const int *type, float side, const f
 /* One engine step with given N(0,1) noise (3 per particle, float values):
  * compensated position (hi, lo), FP64 displacement, reference drift/noise
  * formula with mobility mob[type] and amplitude amp[type]. */
+void or_eng_cap_forces(int n, float *ff, float fcap);
 void or_eng_update(int n, float *hi, float *lo, double *dsp, const float *ff, const int *type, float side,
                    double dt, const float mob[2], const float amp[2], const float *noise);
 float or_eng_amplitude(float temp, float mob, float dt);

@@ -96,6 +96,7 @@ def oracle_lib():
         L.or_eng_forces.argtypes = [C.c_int, _f32p, _i32p, C.c_float, _f32p, _f32p, _f32p, _f32p, _i32p, _u64p]
         L.or_eng_update.argtypes = [C.c_int, _f32p, _f32p, _f64p, _f32p, _i32p, C.c_float, C.c_double, _f32p,
                                     _f32p, _f32p]
+        L.or_eng_cap_forces.argtypes = [C.c_int, _f32p, C.c_float]
         L.or_eng_amplitude.argtypes = [C.c_float, C.c_float, C.c_float]
         L.or_eng_amplitude.restype = C.c_float
         L.or_eng_fself_msd.argtypes = [C.c_int, _f64p, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double)]
@@ -210,6 +211,10 @@ def ref_lib():
         L.ref_cuda_run.argtypes = [P, _f32p, _f32p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float,
                                    C.c_float, C.c_double, _f32p, _f32p, _f32p, _f32p, C.POINTER(C.c_float)]
         L.ref_cuda_run.restype = C.c_int
+        L.ref_cuda_run_sampled.argtypes = [P, _f32p, _f32p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
+                                           C.c_float, C.c_float, C.c_double, C.c_int, _i32p, _f32p, _f32p, _f32p,
+                                           C.POINTER(C.c_float)]
+        L.ref_cuda_run_sampled.restype = C.c_int
         L.ref_cuda_gder.argtypes = [P, _f32p, _f32p, _f32p]
         L.ref_cuda_gder.restype = C.c_int
         L.ref_hst_run.argtypes = [P] + [_f32p] * 10 + [_i32p] * 4 + [C.c_long, C.c_long] + [C.c_float] * 4 + \

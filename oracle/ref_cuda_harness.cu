@@ -128,11 +128,18 @@ int ref_cuda_forces(const parametros *p, const float *rr_big, const float *rr_sm
 /* The reference time loop main.cu:494-588 without the sample-step host work:
  * ni = -ntrans .. niter-1, linear temperature protocol, cuRAND states seeded
  * with idum / idum+1 (main.cu:478-484).  Positions in/out are float3 AoS.
+ * When nsamp > 0, the unwrapped positions rr_raw (big then small) after
+ * sample_after[j] steps from ni = 0 (that is, after the update of step
+ * ni = sample_after[j] - 1, time dt * sample_after[j]) go to
+ * raw_samples + j * 3 * ngrain_tot; sample_after ascending, in 1 .. niter.
  * elapsed_ms: CUDA-event time of the loop.  Returns 0, 1 on cell overflow,
- * 2 on a CUDA error. */
-int ref_cuda_run(const parametros *p, const float *rr_big, const float *rr_sml, int ntrans, int niter, int idum,
-                 float T0, float Tf, float t0, float tf, double dt, float *rr_big_out, float *rr_sml_out,
-                 float *raw_big_out, float *raw_sml_out, float *elapsed_ms) {
+ * 2 on a CUDA error, 3 on a bad sample list. */
+static int ref_cuda_loop(const parametros *p, const float *rr_big, const float *rr_sml, int ntrans, int niter,
+                         int idum, float T0, float Tf, float t0, float tf, double dt, float *rr_big_out,
+                         float *rr_sml_out, float *raw_big_out, float *raw_sml_out, int nsamp,
+                         const int *sample_after, float *raw_samples, float *elapsed_ms) {
+    for (int j = 0; j < nsamp; j++)
+        if (sample_after[j] < 1 || sample_after[j] > niter || (j && sample_after[j] <= sample_after[j - 1])) return 3;
     RefState S; ref_alloc(S, p);
     std::memcpy(S.rr_b, rr_big, S.nb * sizeof(float3)); std::memcpy(S.raw_b, rr_big, S.nb * sizeof(float3));
     std::memcpy(S.rr_s, rr_sml, S.ns * sizeof(float3)); std::memcpy(S.raw_s, rr_sml, S.ns * sizeof(float3));
@@ -146,6 +153,7 @@ int ref_cuda_run(const parametros *p, const float *rr_big, const float *rr_sml, 
     cudaDeviceSynchronize();
     cudaEvent_t e0, e1; cudaEventCreate(&e0); cudaEventCreate(&e1);
     cudaEventRecord(e0);
+    int js = 0;
     for (int ni = -ntrans; ni < niter; ni++) {
         cudaDeviceSynchronize();
         if (ni == 0) {
@@ -157,6 +165,12 @@ int ref_cuda_run(const parametros *p, const float *rr_big, const float *rr_sml, 
         update_ermak_dev<<<S.NB_B, S.NH>>>('b', S.rr_b, S.raw_b, S.ff_b, st_b, S.pars);
         update_ermak_dev<<<S.NB_S, S.NH>>>('s', S.rr_s, S.raw_s, S.ff_s, st_s, S.pars);
         cudaDeviceSynchronize();
+        if (js < nsamp && ni == sample_after[js] - 1) {
+            float *dst = raw_samples + (size_t)js * 3 * (S.nb + S.ns);
+            std::memcpy(dst, S.raw_b, S.nb * sizeof(float3));
+            std::memcpy(dst + 3 * (size_t)S.nb, S.raw_s, S.ns * sizeof(float3));
+            js++;
+        }
         float time = dt * (1.0 + (float)ni);
         S.pars.temp_set = calculate_temp_linear(T0, Tf, t0, tf, time);
         ref_cells_forces(S);
@@ -168,10 +182,26 @@ int ref_cuda_run(const parametros *p, const float *rr_big, const float *rr_sml, 
     int rc = (cudaGetLastError() != cudaSuccess) ? 2 : 0;
     if (!rc && (max_occ(S.nocup_b, S.ncb3) > p->ntags_big || max_occ(S.nocup_s, S.ncs3) > p->ntags_sml)) rc = 1;
     std::memcpy(rr_big_out, S.rr_b, S.nb * sizeof(float3)); std::memcpy(rr_sml_out, S.rr_s, S.ns * sizeof(float3));
-    std::memcpy(raw_big_out, S.raw_b, S.nb * sizeof(float3)); std::memcpy(raw_sml_out, S.raw_s, S.ns * sizeof(float3));
+    if (raw_big_out) std::memcpy(raw_big_out, S.raw_b, S.nb * sizeof(float3));
+    if (raw_sml_out) std::memcpy(raw_sml_out, S.raw_s, S.ns * sizeof(float3));
     cudaFree(st_b); cudaFree(st_s); cudaEventDestroy(e0); cudaEventDestroy(e1);
     ref_free(S);
     return rc;
+}
+
+int ref_cuda_run(const parametros *p, const float *rr_big, const float *rr_sml, int ntrans, int niter, int idum,
+                 float T0, float Tf, float t0, float tf, double dt, float *rr_big_out, float *rr_sml_out,
+                 float *raw_big_out, float *raw_sml_out, float *elapsed_ms) {
+    return ref_cuda_loop(p, rr_big, rr_sml, ntrans, niter, idum, T0, Tf, t0, tf, dt, rr_big_out, rr_sml_out,
+                         raw_big_out, raw_sml_out, 0, nullptr, nullptr, elapsed_ms);
+}
+
+int ref_cuda_run_sampled(const parametros *p, const float *rr_big, const float *rr_sml, int ntrans, int niter,
+                         int idum, float T0, float Tf, float t0, float tf, double dt, int nsamp,
+                         const int *sample_after, float *raw_samples, float *rr_big_out, float *rr_sml_out,
+                         float *elapsed_ms) {
+    return ref_cuda_loop(p, rr_big, rr_sml, ntrans, niter, idum, T0, Tf, t0, tf, dt, rr_big_out, rr_sml_out,
+                         nullptr, nullptr, nsamp, sample_after, raw_samples, elapsed_ms);
 }
 
 /* g(r) histograms of the reference device kernel (main.cu:719-754): the four
