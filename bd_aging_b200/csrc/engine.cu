@@ -324,20 +324,28 @@ int list_rebuild(bd_engine *e, int cur) {
     BD_LAUNCH_CHECK();
     return BD_OK;
 }
-template <int RNG>
-int launch_list_step_t(bd_engine *e, const ListArgs &a, int ni_off) {
+template <int RNG, int V>
+int launch_list_step_v(bd_engine *e, const ListArgs &a, int ni_off) {
+    constexpr int T = ListVariant<V>::kThreads;
     if (e->extra_pot)
-        k_step_list<RNG, true><<<div_up(e->P, BD_LIST_THREADS), BD_LIST_THREADS, 0, e->stream>>>(a, e->d_ni, ni_off);
+        k_step_list<RNG, true, V><<<div_up(e->P, T), T, 0, e->stream>>>(a, e->d_ni, ni_off);
     else
-        k_step_list<RNG, false><<<div_up(e->P, BD_LIST_THREADS), BD_LIST_THREADS, 0, e->stream>>>(a, e->d_ni, ni_off);
+        k_step_list<RNG, false, V><<<div_up(e->P, T), T, 0, e->stream>>>(a, e->d_ni, ni_off);
     BD_LAUNCH_CHECK();
     return BD_OK;
 }
+// every variant for the default (Philox) noise; the compatibility streams
+// run variant 0
 int launch_list_step(bd_engine *e, const ListArgs &a, int ni_off) {
     switch (e->rng) {
-        case BD_RNG_CURAND: return launch_list_step_t<kRngCurand>(e, a, ni_off);
-        case BD_RNG_RANNEW64: return launch_list_step_t<kRngRannew64>(e, a, ni_off);
-        default: return launch_list_step_t<kRngPhilox>(e, a, ni_off);
+        case BD_RNG_CURAND: return launch_list_step_v<kRngCurand, 0>(e, a, ni_off);
+        case BD_RNG_RANNEW64: return launch_list_step_v<kRngRannew64, 0>(e, a, ni_off);
+        default:
+            switch (e->lvar) {
+                case 1: return launch_list_step_v<kRngPhilox, 1>(e, a, ni_off);
+                case 2: return launch_list_step_v<kRngPhilox, 2>(e, a, ni_off);
+                default: return launch_list_step_v<kRngPhilox, 0>(e, a, ni_off);
+            }
     }
 }
 // one list-mode step in phase `cur`: gated rebuild, then the step
@@ -605,6 +613,7 @@ void bd_engine_opts_default(bd_engine_opts *o) {
     o->graph_steps = 96;
     o->qmax = 6.2831853f;
     o->neighbor_skin = 0.25f;
+    o->list_variant = -1;
 }
 
 int bd_engine_create(const bd_system_desc *systems, int nsys, const bd_engine_opts *opts_in, bd_engine **out) {
@@ -635,6 +644,9 @@ int bd_engine_create(const bd_system_desc *systems, int nsys, const bd_engine_op
     e->ni = e->ni_first = opts.ni_start;
     e->rng_stream = opts.rng_stream;
     e->autotune = opts.autotune;
+    if (opts.list_variant < -1 || opts.list_variant >= kListVariants) { delete e; return BD_ERR_ARG; }
+    e->lvar = opts.list_variant >= 0 ? opts.list_variant : 0;
+    e->tune_lvar = opts.list_variant < 0;
     if (!(opts.neighbor_skin >= 0.f) || opts.neighbor_skin > 1.0f) { delete e; return BD_ERR_ARG; }
     // lists serve plain mode with generated noise; a box too small for the
     // enlarged cells keeps the sweep
@@ -768,6 +780,8 @@ int bd_engine_get_info(const bd_engine *e, bd_engine_info *info) {
         info->list_builds = b[0];
         info->list_rebuild_steps = b[1];
     }
+    info->list_variant = e->list ? e->lvar : -1;
+    info->tuned_ms = e->tuned ? e->tuned_ms : 0.f;
     return BD_OK;
 }
 
@@ -874,8 +888,54 @@ int run_direct(bd_engine *e, int k) {
 // persistent mode) on the live batch and keeps the fastest.  The steps it
 // takes are real steps of the run; results do not depend on the layout
 // (every force sum has a fixed order), only the speed does.
+// List mode: the list-step launch variant (unless the caller fixed it) and
+// the brick shape of the list build, timed together on the live batch over
+// whole steps, rebuilds included as they come.  Neither changes a list or a
+// force sum, so the tuned run's results are those of an untuned run.
+int autotune_list(bd_engine *e, long long &nsteps) {
+    static const int shapes[][3] = {{4, 4, 3}, {4, 4, 4}, {3, 3, 3}, {5, 4, 4}, {4, 4, 2}};
+    struct Cand { int bx, by, bz, v; };
+    std::vector<Cand> cands;
+    for (auto &sh : shapes)
+        for (int v = 0; v < kListVariants; v++)
+            if (e->tune_lvar || v == e->lvar) cands.push_back({sh[0], sh[1], sh[2], v});
+    const int warm = 2, timed = 12;
+    if (nsteps < (long long)cands.size() * (warm + timed) + 1) return BD_OK;  // too short to tune now
+    cudaEvent_t t0, t1;
+    BD_CUDA_TRY(cudaEventCreate(&t0));
+    BD_CUDA_TRY(cudaEventCreate(&t1));
+    Cand best = {e->bx, e->by, e->bz, e->lvar};
+    float best_ms = 1e30f;
+    int rc = BD_OK;
+    for (const Cand &c : cands) {
+        e->bx = c.bx; e->by = c.by; e->bz = c.bz; e->lvar = c.v;
+        if (rebuild_bricks(e) != BD_OK) continue;  // staging of this shape does not fit
+        if ((rc = configure_kernels(e)) != BD_OK) break;
+        if ((rc = upload_layout(e)) != BD_OK) break;
+        if ((rc = direct_steps(e, warm)) != BD_OK) break;
+        BD_CUDA_TRY(cudaEventRecord(t0, e->stream));
+        if ((rc = direct_steps(e, timed)) != BD_OK) break;
+        BD_CUDA_TRY(cudaEventRecord(t1, e->stream));
+        if ((rc = engine_status(e)) != BD_OK) break;
+        float ms = 0.f;
+        BD_CUDA_TRY(cudaEventElapsedTime(&ms, t0, t1));
+        nsteps -= warm + timed;
+        if (ms < best_ms) { best_ms = ms; best = c; }
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (rc) return rc;
+    e->bx = best.bx; e->by = best.by; e->bz = best.bz; e->lvar = best.v;
+    if ((rc = rebuild_bricks(e)) != BD_OK) return rc;
+    if ((rc = configure_kernels(e)) != BD_OK) return rc;
+    if ((rc = upload_layout(e)) != BD_OK) return rc;
+    e->tuned = true;
+    e->tuned_ms = best_ms / timed;
+    return BD_OK;
+}
+
 int autotune_layout(bd_engine *e, long long &nsteps) {
-    if (e->list) return BD_OK;  // list steps do not depend on the brick layout
+    if (e->list) return autotune_list(e, nsteps);
     struct Cand { int bx, by, bz, t, cl; };
     static const int shapes[][4] = {{4, 4, 3, 128}, {4, 4, 4, 160}, {5, 4, 4, 192}, {4, 3, 3, 96}, {3, 3, 3, 64},
                                     {4, 4, 2, 96},  {2, 2, 2, 64},  {3, 3, 2, 64},  {6, 4, 3, 192}};

@@ -50,6 +50,8 @@ struct bd_engine {
     cudaGraphExec_t gexec[3] = {nullptr, nullptr, nullptr};  // one per rotation phase e->cur
     int autotune = 0;
     bool tuned = false;
+    int lvar = 0;            // list-step launch variant (ListVariant<lvar>)
+    bool tune_lvar = false;  // the autotuner chooses lvar
     // persistent mode: replicas packed into cluster bins
     std::vector<int> cl_start_h, cl_bricks_h;
     int *d_cl_start = nullptr, *d_cl_bricks = nullptr;

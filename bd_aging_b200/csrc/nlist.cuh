@@ -31,13 +31,19 @@ constexpr int kMaxNbr = 64;
 #ifndef BD_LIST_GATHER
 #define BD_LIST_GATHER 4  // list partners whose positions are in flight together
 #endif
-#ifndef BD_LIST_THREADS
-#define BD_LIST_THREADS 128  // CTA size of the list step
-#endif
-#ifndef BD_LIST_MINB
-#define BD_LIST_MINB 8       // resident CTAs per SM asked of the register allocator (64 registers)
-#endif
 constexpr int kGather = BD_LIST_GATHER;
+// Launch variants of the list step, chosen per engine by the autotuner:
+// CTA size, resident CTAs per SM asked of the register allocator (8 x 128
+// threads: 64 registers; 9 x 128: 56), and whether the particle's own state
+// (remainder, build position, reference index) is loaded before the force
+// loop (its latency hidden under the gathers) or after it (fewer registers
+// live in the loop).  Each particle's arithmetic is the same in every
+// variant, so results do not depend on the choice.
+template <int V> struct ListVariant;
+template <> struct ListVariant<0> { static constexpr int kThreads = 128, kMinBlocks = 8; static constexpr bool kLate = false; };
+template <> struct ListVariant<1> { static constexpr int kThreads = 256, kMinBlocks = 4; static constexpr bool kLate = false; };
+template <> struct ListVariant<2> { static constexpr int kThreads = 128, kMinBlocks = 9; static constexpr bool kLate = true; };
+constexpr int kListVariants = 3;
 constexpr int kListBuildThreads = 256;  // CTA size of the list build
 static_assert(kGather % 2 == 0 && kMaxNbr % kGather == 0, "partners are paired for f32x2 arithmetic");
 
@@ -418,9 +424,9 @@ __device__ __forceinline__ void list_forces_extra(const ListArgs &a, const SysDe
 // displacement exactly as process_brick.
 // EXTRA: some replica of the batch uses a potential other than the modified
 // WCA (instantiated separately so the default kernel keeps its registers).
-template <int RNG, bool EXTRA>
-__global__ void __launch_bounds__(BD_LIST_THREADS, BD_LIST_MINB) k_step_list(ListArgs a, const long long *ni_base,
-                                                                          int ni_off) {
+template <int RNG, bool EXTRA, int V>
+__global__ void __launch_bounds__(ListVariant<V>::kThreads, ListVariant<V>::kMinBlocks)
+    k_step_list(ListArgs a, const long long *ni_base, int ni_off) {
     const int sid = blockIdx.x * blockDim.x + threadIdx.x;
     if (sid >= a.np) return;
     const long long ni = *ni_base + ni_off;
@@ -432,10 +438,14 @@ __global__ void __launch_bounds__(BD_LIST_THREADS, BD_LIST_MINB) k_step_list(Lis
     const int tm = (int)(wi >> 31);
     const float sg0 = tm ? S.sig[1] : S.sig[0], sg1 = tm ? S.sig[2] : S.sig[1];
     const float c0 = tm ? S.cut2[1] : S.cut2[0], c1 = tm ? S.cut2[2] : S.cut2[1];
-    // own state early: its latency overlaps the force loop
-    const int gid = __ldg(a.gid_of + sid);
-    float lx = a.lo_x[sid], ly = a.lo_y[sid], lz = a.lo_z[sid];
-    const float4 pb = __ldg(a.pbuild + sid);
+    int gid;
+    float lx, ly, lz;
+    float4 pb;
+    if constexpr (!ListVariant<V>::kLate) {  // own state early: its latency overlaps the force loop
+        gid = __ldg(a.gid_of + sid);
+        lx = a.lo_x[sid], ly = a.lo_y[sid], lz = a.lo_z[sid];
+        pb = __ldg(a.pbuild + sid);
+    }
     float fx, fy, fz;
     const int n = min(__ldg(a.nnb + sid), kMaxNbr);
     if (EXTRA && S.pot != kPotWcaModified) {
@@ -463,6 +473,11 @@ __global__ void __launch_bounds__(BD_LIST_THREADS, BD_LIST_MINB) k_step_list(Lis
         } else if (!isfinite(fmx)) {
             fx = fy = fz = 0.f;
         }
+    }
+    if constexpr (ListVariant<V>::kLate) {
+        gid = __ldg(a.gid_of + sid);
+        lx = a.lo_x[sid], ly = a.lo_y[sid], lz = a.lo_z[sid];
+        pb = __ldg(a.pbuild + sid);
     }
     const int pid = gid - S.part_base;
     if (ni == 0) {  // origin of the unwrapped positions (main.cu:497-506)

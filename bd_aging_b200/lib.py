@@ -60,7 +60,7 @@ class EngineOpts(C.Structure):
     _fields_ = [("rng", C.c_int), ("cell_capacity", C.c_int), ("brick", C.c_int * 3), ("threads", C.c_int),
                 ("mode", C.c_int), ("cluster", C.c_int), ("autotune", C.c_int), ("graph_steps", C.c_int),
                 ("qmax", C.c_float), ("ni_start", C.c_longlong), ("rng_stream", C.c_uint),
-                ("neighbor_skin", C.c_float)]
+                ("neighbor_skin", C.c_float), ("list_variant", C.c_int)]
 
 
 class Observables(C.Structure):
@@ -86,7 +86,8 @@ class EngineInfo(C.Structure):
                 ("brick", C.c_int * 3), ("threads", C.c_int), ("cell_capacity", C.c_int),
                 ("staging_capacity", C.c_int), ("mode", C.c_int), ("cluster", C.c_int),
                 ("smem_bytes", C.c_size_t), ("next_step", C.c_longlong), ("neighbor_skin", C.c_float),
-                ("list_builds", C.c_longlong), ("list_rebuild_steps", C.c_longlong)]
+                ("list_builds", C.c_longlong), ("list_rebuild_steps", C.c_longlong), ("list_variant", C.c_int),
+                ("tuned_ms", C.c_float)]
 
 
 _LIB = None
@@ -374,7 +375,7 @@ class Engine:
 
     def __init__(self, systems, rng="philox", mode="auto", brick=None, threads=0, cell_capacity=0,
                  graph_steps=96, qmax=2 * np.pi, ni_start=0, rng_stream=0, cluster=0, autotune=0,
-                 neighbor_skin=None):
+                 neighbor_skin=None, list_variant=None):
         self.systems = list(systems)
         n = len(self.systems)
         arr = (SystemDesc * n)(*[s.desc() for s in self.systems])
@@ -394,6 +395,8 @@ class Engine:
         o.autotune = autotune
         if neighbor_skin is not None:  # None: the library default
             o.neighbor_skin = neighbor_skin
+        if list_variant is not None:  # None: the library default (tuned when autotune is set)
+            o.list_variant = list_variant
         h = _vp()
         _check(_lib().bd_engine_create(arr, n, C.byref(o), C.byref(h)), "bd_engine_create")
         self._h = h

@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define BD_ABI_VERSION 1
+#define BD_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------ */
 #define BD_OK                 0
@@ -280,7 +280,12 @@ typedef struct bd_engine_opts {
                                   generated noise): lists of partners within cut + skin,
                                   rebuilt on the device when a particle of the replica
                                   has moved skin / 2; 0: the 27-cell sweep every step */
+    int list_variant;          /* list-step launch variant 0 .. BD_LIST_VARIANTS-1 (CTA size,
+                                  registers, load placement; same results), or -1 (default):
+                                  variant 0, or with autotune chosen with the brick shape
+                                  at the first run */
 } bd_engine_opts;
+#define BD_LIST_VARIANTS 3
 
 typedef struct bd_observables {
     double energy_big, energy_sml; /* (1/N) sum 0.5 pot_i per species (main.cu:627-631) */
@@ -300,6 +305,8 @@ typedef struct bd_engine_info {
     float neighbor_skin;          /* 0 when the engine sweeps every step */
     long long list_builds;        /* neighbour-list builds so far (per replica) */
     long long list_rebuild_steps; /* time steps that rebuilt some replica's lists */
+    int list_variant;             /* list-step launch variant in use (-1: sweep mode) */
+    float tuned_ms;               /* autotuner: time per step of the chosen layout (0 untuned) */
 } bd_engine_info;
 
 void bd_engine_opts_default(bd_engine_opts *opts);

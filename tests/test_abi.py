@@ -32,7 +32,7 @@ def test_library_exports_every_declared_symbol():
     assert len(names) > 20
     missing = [n for n in names if not hasattr(L, n)]
     assert not missing, missing
-    assert L.bd_abi_version() == 1
+    assert L.bd_abi_version() == 2
 
 
 def test_status_strings():

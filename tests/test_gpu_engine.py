@@ -206,3 +206,35 @@ def test_autotuner_changes_speed_not_results():
         e1.set_positions(pos)
         e1.run(300)
         np.testing.assert_array_equal(ea.get_positions()[0], e1.get_positions()[0])
+
+
+def test_list_autotuner_and_launch_variants_change_speed_not_results():
+    """List mode: every list-step launch variant, and the autotuner's choice
+    of variant and build brick (timed on the live batch), give the same bits
+    as the default layout."""
+    systems, poss = _ragged(4, 71)
+    pos = np.concatenate(poss)
+    ref = B.Engine(list(systems))
+    assert ref.info().neighbor_skin > 0 and ref.info().list_variant == 0
+    ref.set_positions(pos)
+    ref.run(400)
+    want = ref.get_positions()
+    for v in (1, 2):
+        ev = B.Engine(list(systems), list_variant=v)
+        assert ev.info().list_variant == v
+        ev.set_positions(pos)
+        ev.run(400)
+        got = ev.get_positions()
+        np.testing.assert_array_equal(got[0], want[0])
+        np.testing.assert_array_equal(got[1], want[1])
+        ev.close()
+    ea = B.Engine(list(systems), autotune=1)
+    ea.set_positions(pos)
+    ea.run(400)  # 15 candidates x 14 steps are timed inside the first call
+    info = ea.info()
+    assert info.tuned_ms > 0 and 0 <= info.list_variant < 3
+    got = ea.get_positions()
+    np.testing.assert_array_equal(got[0], want[0])
+    np.testing.assert_array_equal(got[1], want[1])
+    with pytest.raises(B.BDError):
+        B.Engine(list(systems), list_variant=3)
