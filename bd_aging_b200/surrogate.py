@@ -32,11 +32,14 @@ G_RANGE = (0.8, 2.4)  # r window of the g(r) features, in units of the small ref
 
 # ------------------------------------------------------------------ data
 def make_systems(settings, n_per_replica=1000, dt=1e-4, seed=1):
-    """One replica per (phi, T_final): 50:50 mixture quenched from T0 = 1.0
-    to T_final at t = 0 (instantaneous: tf = t0 + 1e-30)."""
+    """One replica per (phi, T_final) or (phi, T_final, N): 50:50 mixture
+    quenched from T0 = 1.0 to T_final at t = 0 (instantaneous: tf = t0 +
+    1e-30), N = n_per_replica unless the setting gives it."""
     out = []
-    for i, (phi, tfin) in enumerate(settings):
-        nb = ns = n_per_replica // 2
+    for i, st in enumerate(settings):
+        phi, tfin = st[0], st[1]
+        n = int(st[2]) if len(st) > 2 else n_per_replica
+        nb = ns = n // 2
         side = float(np.float32(CF.side_from_phi(nb, ns, float(phi))))
         out.append(B.System(n_big=nb, n_sml=ns, side=side, sigma_big=float(CF.SIGMA_BIG),
                             sigma_sml=float(CF.SIGMA_SML), dt=dt, T0=1.0, Tf=float(tfin), t0=0.0, tf=1e-30,
@@ -106,7 +109,8 @@ def simulate(settings, t_ws, lags, ks, n_per_replica=1000, dt=1e-4, trans_steps=
             c = e.correlate(slots, float(q))
             for j, (k, lag) in enumerate(events[stop]):
                 tw_t, lag_t = max(tw_steps[k], 1) * dt, lag * dt
-                for r, (phi, tfin) in enumerate(settings):
+                for r, st in enumerate(settings):
+                    phi, tfin = st[0], st[1]
                     msd = max(float(c[j, r]["msd_big"]), 1e-12)
                     rows_x.append([phi, tfin, math.log10(tw_t), math.log10(lag_t), q])
                     rows_y.append(np.concatenate([[c[j, r]["fself_big"], math.log10(msd)], gf[r]]))
@@ -277,10 +281,48 @@ def seed_average(X, Y):
     return keys.astype(np.float32), (ys / cnt).astype(np.float32)
 
 
-def held_out_fs_error(model, phis, temps, seeds=4, n_per_replica=1000, dt=1e-4, seed=777):
+def held_out_fs_error(model, phis, temps, seeds=4, n_per_replica=1000, dt=1e-4, seed=777, t_ws=TRAIN_TW,
+                      lags=TRAIN_LAGS, ks=TRAIN_KS):
     """Mean and max |F_s(predicted) - F_s(simulated)| over plain runs at
     settings the model has not seen (seed-averaged simulations)."""
-    X, Y = build_dataset(phis, temps, seeds, n_per_replica=n_per_replica, dt=dt, seed=seed)
+    X, Y = build_dataset(phis, temps, seeds, t_ws=t_ws, lags=lags, ks=ks, n_per_replica=n_per_replica, dt=dt,
+                         seed=seed)
     Xa, Ya = seed_average(X, Y)
     err = np.abs(model.predict(Xa)[:, 0] - Ya[:, 0])
     return float(err.mean()), float(err.max()), len(Xa)
+
+
+# ------------------------------------------------------------------ batched-run data
+# Training data from one ragged batch of replicas like the batched workload:
+# N uniform in [500, 8000], phi uniform in [0.50, 0.60], T_final uniform in
+# [0.05, 1.0], dt = 1e-5, instantaneous quench from T0 = 1.0; 16 waiting
+# times log-spaced over two decades and 8 lags log-spaced over three decades
+# (in steps), three wave numbers: 256 replicas give about 1e5 samples.
+BATCH_DT = 1e-5
+BATCH_TW = tuple(int(v) for v in np.unique(np.geomspace(100, 10000, 16).astype(int)))
+BATCH_LAGS = tuple(int(v) for v in np.unique(np.geomspace(10, 10000, 8).astype(int)))
+BATCH_KS = (5.0, 7.0, 9.0)
+
+
+def ragged_settings(replicas, seed):
+    """(phi, T_final, N) of `replicas` replicas drawn like the batched workload."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(replicas):
+        n = int(rng.integers(500, 8001)) // 2 * 2
+        out.append((float(rng.uniform(0.50, 0.60)), float(rng.uniform(0.05, 1.0)), n))
+    return out
+
+
+def build_batched_dataset(replicas=256, seed=11, t_ws=BATCH_TW, lags=BATCH_LAGS, ks=BATCH_KS, dt=BATCH_DT):
+    """Training rows from one ragged batched run (one row per replica, t_w,
+    lag and wave number)."""
+    return simulate(ragged_settings(replicas, seed), list(t_ws), list(lags), list(ks), dt=dt, seed=seed)
+
+
+def held_out_batched_fs_error(model, phis=(0.525, 0.575), temps=(0.2, 0.45, 0.7, 0.9), seeds=4, n=4000,
+                              seed=777):
+    """held_out_fs_error on plain runs of N = n at fixed (phi, T_final)
+    settings, over the batched data's windows and wave numbers."""
+    return held_out_fs_error(model, phis, temps, seeds=seeds, n_per_replica=n, dt=BATCH_DT, seed=seed,
+                             t_ws=BATCH_TW, lags=BATCH_LAGS, ks=BATCH_KS)

@@ -35,6 +35,8 @@ sys.path.insert(0, ROOT)
 
 METRIC = "particle-steps/s on 1 B200, batched vs plain, at matched g(r)/F_s error"
 ALG_BYTES_PER_PARTICLE_STEP = 96  # FP32 position + remainder (24 B) and FP64 displacement (24 B), read + write
+FLOP_PER_PAIR = 30                # FP32 work of one interacting pair force
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
 
 def parse():
@@ -60,6 +62,8 @@ def parse():
     ap.add_argument("--autotune", action="store_true", help="time brick shapes during warm-up, keep the fastest")
     ap.add_argument("--skin", type=float, default=None,
                     help="neighbour-list skin (0: sweep every step; default: the library's)")
+    ap.add_argument("--list-variant", type=int, default=None,
+                    help="list-step launch variant (default: the library's; chosen by --autotune)")
     return ap.parse_args()
 
 
@@ -198,17 +202,19 @@ def cuda_time(engine, fn, iters):
     return e0.elapsed_time(e1)  # ms
 
 
-def cpu_baseline(seconds=12.0):
+def cpu_baseline(pos=None, seconds=12.0):
     """Reference host implementation (oracle/_ref) on one N=32768 phi=0.58
-    replica, single thread (the reference's *_hst functions keep state in
-    static locals), bounded sample."""
+    replica of the timed batch (its relaxed start state `pos`; a jittered
+    lattice when none is given), single thread (the reference's *_hst
+    functions keep state in static locals), bounded sample."""
     from oracle import oracle as O
     from bd_aging_b200 import configs as CF
     if not O.ref_available():
         return None
     nb = ns = 16384
     side = float(np.float32(CF.side_from_phi(nb, ns, 0.58)))
-    pos = CF.lattice_config(nb, ns, side, 99, jitter=0.05)
+    if pos is None:
+        pos = CF.lattice_config(nb, ns, side, 99, jitter=0.05)
     p = O.setup_params(side, nb, ns, float(CF.SIGMA_BIG), float(CF.SIGMA_SML), ntags=(16, 16), nbins=400,
                        rng=side / 2, dt=1e-5, T0=1.0)
     run = O.RefHostRun(p, pos)
@@ -220,7 +226,8 @@ def cpu_baseline(seconds=12.0):
     run.run(n, 1.0, 0.1, 0.0, 1e-30, 1e-5)
     el = time.perf_counter() - t
     return {"value": 32768 * n / el, "unit": "particle-steps/s", "cores": 1, "kind": "reference",
-            "sample": "%d steps of one N=32768 phi=0.58 replica, reference host loop (oracle/_ref)" % n}
+            "sample": "%d steps of replica 0 of the timed batch (N=32768 phi=0.58, relaxed start), reference "
+                      "host loop (oracle/_ref)" % n}
 
 
 def reference_cuda(steps=200):
@@ -365,22 +372,78 @@ def surrogate_leg(steps=200, warmup=20, batch=4096):
 
 
 def surrogate_quality_leg():
-    """The surrogate trained on engine runs (phi in {0.50, 0.55, 0.60} x 8
-    T_final x 8 seeds, 4 waiting times x 12 lags x 5 wave numbers: 46k samples,
-    4000 Adam steps) and its F_s error on plain runs at unseen settings
+    """The surrogate trained on one ragged batched engine run (256 replicas,
+    N in [500, 8000], phi in [0.50, 0.60], T_final in [0.05, 1.0], dt = 1e-5,
+    16 waiting times x 8 lags x 3 wave numbers: about 1e5 samples, 4000 Adam
+    steps) and its F_s error on plain N = 4000 runs at unseen settings
     (phi in {0.525, 0.575} x T_final in {0.2, 0.45, 0.7, 0.9}, 4 seeds each)."""
     from bd_aging_b200 import surrogate as S
     t0 = time.perf_counter()
-    X, Y = S.build_dataset(phis=(0.50, 0.55, 0.60), temps=np.linspace(0.05, 1.0, 8), seeds=8)
+    X, Y = S.build_batched_dataset(replicas=256, seed=11)
     t1 = time.perf_counter()
     model = S.SurrogateModel(seed=3)
     loss = model.fit(X, Y, steps=4000, lr=1e-3)
     t2 = time.perf_counter()
-    mean_err, max_err, n = S.held_out_fs_error(model, phis=(0.525, 0.575), temps=(0.2, 0.45, 0.7, 0.9))
+    mean_err, max_err, n = S.held_out_batched_fs_error(model)
     model.close()
     return {"train_samples": int(len(X)), "final_loss": loss, "held_out_points": n,
             "held_out_fs_mean_abs_err": mean_err, "held_out_fs_max_abs_err": max_err,
+            "data": "256 ragged replicas, dt=1e-5, t_w 1e-3..1e-1, lags 1e-4..1e-1, k in {5, 7, 9}",
+            "held_out": "plain N=4000 runs, phi {0.525, 0.575} x T_final {0.2, 0.45, 0.7, 0.9}, 4 seeds",
             "data_generation_s": t1 - t0, "training_s": t2 - t1}
+
+
+def workload_leg(name, steps=3, warmup=2, md_steps=960, autotune=False):
+    """Throughput of another BASELINE configuration on its own engine (same
+    timing as the headline: CUDA events around `steps` runs of `md_steps` time
+    steps after `warmup` runs, inputs resident).  "large" also reports the
+    rate with its g(r) sample every 100 steps (config 4)."""
+    from bd_aging_b200 import lib as B
+    systems, desc = workload_systems(name, 64, 0)
+    pos = relaxed_positions(systems, 777, 2000)
+    P = sum(s.n for s in systems)
+    eng = B.Engine(systems, graph_steps=96, autotune=int(autotune))
+    eng.set_positions(pos)
+    for _ in range(warmup):
+        eng.run(md_steps)
+    info0 = eng.info()
+    ms = cuda_time(eng, lambda: eng.run(md_steps), steps)
+    info = eng.info()
+    out = dict(desc, value=P * md_steps * steps / (ms / 1e3), unit="particle-steps/s", particles=P,
+               md_steps_per_bench_step=md_steps, ms_per_step=ms / steps, steps=steps, warmup=warmup,
+               list_rebuild_steps_timed=int(info.list_rebuild_steps - info0.list_rebuild_steps),
+               autotune=bool(autotune), brick=list(info.brick), list_variant=info.list_variant)
+    if name == "large":  # g(r) every 100 steps, 400 bins to r = 15 (the cell stencil at this size)
+        import torch
+        eng.gder(400, 15.0)
+        st = torch.cuda.ExternalStream(eng.stream_handle())
+        t0 = time.perf_counter()
+        eng.gder(400, 15.0)
+        st.synchronize()
+        tg = time.perf_counter() - t0
+        t100 = 100 * (ms / 1e3) / (md_steps * steps)
+        out["gder_ms_per_sample"] = tg * 1e3
+        out["value_with_gder_every_100_steps"] = P * 100 / (t100 + tg)
+    eng.close()
+    return out
+
+
+def statistics_leg(seeds=8):
+    """Long-run agreement with the reference's own CUDA build at the aging
+    workload's conditions (N = 32768, phi = 0.58, quench 1.0 -> 0.1, dt =
+    1e-5, 2000 steps): 8 noise seeds of each from the same 8 relaxed states;
+    MSD and F_s (k = 7) at 4 times and g(r) (400 bins to r = 15) compared
+    through the seed-to-seed standard errors (oracle/statistics.py)."""
+    from oracle import oracle as O
+    from oracle import statistics as ST
+    if not O.ref_available():
+        return None
+    r = ST.run(ST.AGING, seeds=seeds)
+    obs = {o: {"t": r["times"][-1], "engine": v["engine"][-1], "reference": v["reference"][-1],
+               "se": v["se"][-1], "max_abs_z_over_times": max(abs(z) for z in v["z"])}
+           for o, v in r["observables"].items()}
+    return {"workload": r["case"], "seeds": seeds, "observables": obs, "max_abs_z": r["max_abs_z"],
+            "gder": r["gder"], "engine_s": r["engine_s"], "reference_s": r["reference_s"]}
 
 
 _RELAXED_CACHE = {}
@@ -430,7 +493,8 @@ def run_ours(args):
     P = sum(s.n for s in systems)
     S = args.md_steps
     eng = B.Engine(systems, graph_steps=96, brick=args.brick, threads=args.threads, mode=args.mode,
-                   cluster=args.cluster, autotune=int(args.autotune), neighbor_skin=args.skin)
+                   cluster=args.cluster, autotune=int(args.autotune), neighbor_skin=args.skin,
+                   list_variant=args.list_variant)
     eng.set_positions(pos)
     for _ in range(args.warmup):
         eng.run(S)
@@ -443,6 +507,10 @@ def run_ours(args):
     ranks.barrier()
     ck = clocks.stop()
     rebuild_steps = eng.info().list_rebuild_steps - info.list_rebuild_steps
+    # interacting partners per particle in the timed state (each ordered pair
+    # once per particle), for the FP32 work of the pair forces
+    nbr_count, _ = eng.census()
+    pairs = float(nbr_count.astype(np.int64).sum())
     total_ps = P * S * args.steps * world
     value = total_ps / (ms / 1e3)
     launches = S * args.steps
@@ -467,6 +535,7 @@ def run_ours(args):
                            brick=list(info.brick), threads=info.threads, cell_capacity=info.cell_capacity,
                            mode=args.mode, cluster=info.cluster if args.mode == "persistent" else None,
                            neighbor_skin=info.neighbor_skin, list_builds=info.list_builds,
+                           list_variant=info.list_variant,
                            list_rebuild_steps_timed=int(rebuild_steps),
                            autotune=bool(args.autotune)),
             "gpu_launches": int(gpu_launches),
@@ -474,7 +543,14 @@ def run_ours(args):
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "alg_bytes_per_launch": ALG_BYTES_PER_PARTICLE_STEP * P,
                          "traffic": (tpp * P) if tpp else None},
-            "clocks": ck}
+            "clocks": ck,
+            # secondary roofline (pair forces on the FP32 pipes): 30 FLOP per
+            # interacting ordered pair; nominal FP32 peak 148 SMs x 128 lanes
+            # x 2 FLOP x 1.965 GHz
+            "fp32": {"flop_per_launch": FLOP_PER_PAIR * pairs, "interacting_pairs_per_particle": pairs / P,
+                     "achieved_tflops": FLOP_PER_PAIR * pairs / avg_launch_s / 1e12,
+                     "peak_tflops": FP32_PEAK_TFLOPS, "peak_kind": "nominal",
+                     "frac": FLOP_PER_PAIR * pairs / avg_launch_s / 1e12 / FP32_PEAK_TFLOPS}}
     if rank == 0 and world == 1 and args.only_leg:
         if args.only_leg == "correlator":
             line["correlator"] = correlator_leg(eng, P)
@@ -514,11 +590,21 @@ def run_ours(args):
                 line["batched_over_reference_cuda"] = value / line["reference_cuda"]["value"]
         except Exception as ex:  # reported, never fatal for the bench line
             line["reference_cuda"] = {"error": str(ex)[:200]}
-        line["cpu_baseline"] = cpu_baseline()
+        line["cpu_baseline"] = cpu_baseline(pos[:32768] if args.workload == "aging" else None)
         line["gder"] = gder_leg(eng, systems)
         line["correlator"] = correlator_leg(eng, P)
         eng.close()
+        line["workloads"] = {}
+        for wl in ("batched", "large", "small"):  # BASELINE configs 3, 4 and 1 beside the headline (config 2)
+            try:
+                line["workloads"][wl] = workload_leg(wl, autotune=(wl == "batched"))
+            except Exception as ex:  # reported, never fatal for the bench line
+                line["workloads"][wl] = {"error": str(ex)[:200]}
         line["precision"] = precision_leg()
+        try:
+            line["statistics"] = statistics_leg()
+        except Exception as ex:  # reported, never fatal for the bench line
+            line["statistics"] = {"error": str(ex)[:200]}
         line["surrogate"] = surrogate_leg()
         line["surrogate_quality"] = surrogate_quality_leg()
     eng.close()
@@ -529,13 +615,12 @@ def run_ours(args):
 
 # ------------------------------------------------------------ reference arm
 def _ref_worker(args_tuple):
-    nsteps, reps, seed = args_tuple
+    nsteps, reps, seed, pos = args_tuple
     sys.path.insert(0, ROOT)
     from oracle import oracle as O
     from bd_aging_b200 import configs as CF
     nb = ns = 16384
     side = float(np.float32(CF.side_from_phi(nb, ns, 0.58)))
-    pos = CF.lattice_config(nb, ns, side, seed, jitter=0.05)
     p = O.setup_params(side, nb, ns, float(CF.SIGMA_BIG), float(CF.SIGMA_SML), ntags=(16, 16), nbins=400,
                        rng=side / 2, dt=1e-5, T0=1.0)
     run = O.RefHostRun(p, pos, seed)
@@ -545,11 +630,29 @@ def _ref_worker(args_tuple):
     return time.perf_counter() - t
 
 
+def reference_start_states(count):
+    """The GPU arm's start states: replicas 0 .. count-1 of the aging batch
+    (uniform random positions relaxed by 2000 capped-force steps, seed 777),
+    made before any timing; without a GPU, jittered lattices."""
+    from bd_aging_b200 import configs as CF
+    try:
+        import torch
+        if torch.cuda.is_available():
+            systems, _ = workload_systems("aging", max(64, count), 0)
+            pos = relaxed_positions(systems, 777, 2000)
+            return [pos[k * 32768:(k + 1) * 32768].copy() for k in range(count)], "relaxed"
+    except Exception:
+        pass
+    side = float(np.float32(CF.side_from_phi(16384, 16384, 0.58)))
+    return [CF.lattice_config(16384, 16384, side, 11 + k, jitter=0.05) for k in range(count)], "lattice"
+
+
 def run_reference(args):
     """The reference's own CPU implementation (host functions compiled from its
     sources, oracle/_ref) on every host core: one independent N=32768 replica
     per process (its functions are not reentrant), each bench step a bounded
-    sample of 2 time steps per replica."""
+    sample of 2 time steps per replica.  The replicas start from the GPU arm's
+    relaxed states (replicas 0 .. cores-1 of its batch)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -564,19 +667,23 @@ def run_reference(args):
         cores = os.cpu_count() or 1
     per = 2
     ctx = mp.get_context("spawn")
-    with ctx.Pool(cores) as pool:
-        pool.map(_ref_worker, [(per, max(1, args.warmup // 3), 11 + k) for k in range(cores)])
+    with ctx.Pool(cores) as pool:  # started before the first GPU call
+        states, kind = reference_start_states(cores)
+        pool.map(_ref_worker, [(per, max(1, args.warmup // 3), 11 + k, states[k]) for k in range(cores)])
         t = time.perf_counter()
-        times = pool.map(_ref_worker, [(per, args.steps, 11 + k) for k in range(cores)])
+        pool.map(_ref_worker, [(per, args.steps, 11 + k, states[k]) for k in range(cores)])
         wall = time.perf_counter() - t
     total = 32768 * per * args.steps * cores
     value = total / wall
     line = {"metric": METRIC, "impl": "reference", "value": value, "unit": "particle-steps/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic: jittered lattice at phi=0.58",
+            "data": ("synthetic: the GPU arm's start states (uniform random positions relaxed by 2000 capped-force "
+                     "steps, made before timing)" if kind == "relaxed" else "synthetic: jittered lattice"),
             "config": {"workload": "aging quench N=32768 phi=0.58 T 1.0->0.1 dt=1e-5, one replica per host core",
-                       "replicas": cores, "md_steps_per_bench_step": per},
+                       "replicas": cores, "md_steps_per_bench_step": per,
+                       "replicas_note": "one replica per host core (the reference's host functions are not "
+                                        "reentrant); the GPU arm batches 64"},
             "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores, "kind": "reference",
                              "sample": "%d replicas x %d steps per bench step, reference host loop" % (cores, per)},
             "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
