@@ -13,7 +13,10 @@
 //  * msd_averaged.out holds the last configuration's MSD (main.cu:795-797
 //    assigns instead of accumulating), the other files are averages;
 //  * "log" sampling follows the LOG_SAMPLE build (main.cu:169-173, 612-616),
-//    "linear" sampling the default build (main.cu:618-619).
+//    "linear" sampling the default build (main.cu:618-619);
+//  * configurations after the first take their first step at the temperature
+//    the previous configuration ended on (temp_set is set to T0 once,
+//    main.cu:156, before the loop over configurations).
 // Deviations: out-of-box input coordinates are wrapped into the box (the
 // reference indexes cells out of bounds); bounds are checked where the
 // reference reads past its arrays (main.cu:613).
@@ -206,6 +209,16 @@ int main() {
     // engine: one replica per configuration, all from the first file's geometry
     const char *rng_env = getenv("BD_RNG");
     const bool philox = rng_env && !strcmp(rng_env, "philox");
+    // The reference sets temp_set to T0 once, before its loop over
+    // configurations (main.cu:156), and updates it after every step
+    // (main.cu:520-524): every configuration after the first starts at the
+    // temperature the previous one ended on, after its last step niter - 1.
+    float T_carry = T0;
+    if (niter > -ntrans) {
+        const float t_last = (float)(dt * (1.0 + (float)(niter - 1)));
+        if (!strcmp(protocol, "linear")) T_carry = bd_calculate_temp_linear(T0, Tf, t0, tf, t_last);
+        else if (!strcmp(protocol, "sine")) T_carry = bd_calculate_temp_sine(T0, Tf, t0, tf, period, t_last);
+    }
     std::vector<bd_system_desc> desc(n_configs);
     for (int i = 0; i < n_configs; i++) {
         bd_system_desc &d = desc[i];
@@ -217,6 +230,10 @@ int main() {
         d.temp_protocol = !strcmp(protocol, "sine") ? BD_PROTOCOL_SINE : BD_PROTOCOL_LINEAR;
         d.T0 = T0; d.Tf = Tf; d.t0 = t0; d.tf = tf; d.period = period;
         d.seed = philox ? (unsigned long long)idum * 1000003ull + i : (unsigned long long)(long long)idum;
+        if (i > 0) {
+            d.first_temp_set = 1;
+            d.T_first = T_carry;
+        }
     }
     bd_engine_opts opts;
     bd_engine_opts_default(&opts);

@@ -318,9 +318,9 @@ int list_rebuild(bd_engine *e, int cur) {
     cudaStream_t st = e->stream;
     int rc = list_bin(e, cur, e->lflag + e->R, e->lflag);
     if (rc) return rc;
-    ListBuild lb{e->nbr, e->nnb, e->pbuild, e->lpos[cur & 1], e->lflag, e->R};
+    ListBuild lb{e->nbr, e->nnb, e->pbuild, e->lpos[cur & 1], e->lflag, e->R, e->d_builds,
+                 reinterpret_cast<unsigned *>(e->d_builds + 2)};
     k_list_build<<<rebuild_grid(e, e->nbricks), kListBuildThreads, e->lsmem, st>>>(make_args(e, 0, 0), lb);
-    k_list_done<<<1, 256, 0, st>>>(e->lflag, e->R, e->d_builds);
     BD_LAUNCH_CHECK();
     return BD_OK;
 }
@@ -590,6 +590,7 @@ int setup_geometry(bd_engine *e) {
         S.fcap = d.force_cap;
         S.protocol = d.temp_protocol;
         S.T0 = d.T0; S.Tf = d.Tf; S.t0 = d.t0; S.tf = d.tf; S.period = d.period;
+        S.T_first = d.first_temp_set ? d.T_first : d.T0;
         S.seed = d.seed;
         cell_base += (long long)nc * nc * nc;
         part_base += S.n;
@@ -716,8 +717,8 @@ int bd_engine_create(const bd_system_desc *systems, int nsys, const bd_engine_op
         ALLOC(e->amp_tab, sizeof(float) * 2 * (size_t)e->R * e->graph_steps);
         ALLOC(e->lflag, sizeof(int) * (e->R + 1));
         ALLOC(e->d_one, sizeof(int));
-        ALLOC(e->d_builds, 2 * sizeof(long long));
-        cudaMemsetAsync(e->d_builds, 0, 2 * sizeof(long long), e->stream);
+        ALLOC(e->d_builds, 3 * sizeof(long long));  // + the build's finished-block counter
+        cudaMemsetAsync(e->d_builds, 0, 3 * sizeof(long long), e->stream);
         const int one = 1;
         cudaMemcpyAsync(e->d_one, &one, sizeof(int), cudaMemcpyHostToDevice, e->stream);
     }
@@ -794,10 +795,13 @@ int bd_engine_get_stream(const bd_engine *e, void **stream) {
 int bd_engine_set_positions(bd_engine *e, const float *pos) {
     if (!e || !pos) return BD_ERR_ARG;
     const size_t P = (size_t)e->P;
-    // storage order: replica, brick, cell within brick, reference index --
-    // computed on the device (keys, counting sort over the slots, per-slot
-    // sort by reference index)
-    const long long V = (long long)e->bx * e->by * e->bz, T = (long long)e->nbricks * V;
+    // storage order: replica, brick, species, cell within brick, reference
+    // index -- computed on the device (keys, counting sort over the slots,
+    // per-slot sort by reference index).  Inside a cell the order is that of
+    // the reference index either way (big particles come first), so the
+    // species split changes no sweep or list order; it gives the list step
+    // warps of one species, whose list lengths are alike.
+    const long long V = (long long)e->bx * e->by * e->bz, T = (long long)e->nbricks * V * 2;
     if (T > INT_MAX) return BD_ERR_ARG;
     if (!e->ld_in) {
         BD_CUDA_TRY(cudaMalloc(&e->ld_in, sizeof(float) * 3 * P));

@@ -34,6 +34,7 @@ struct SysDev {
     double dt_d;
     int protocol;           // 0 linear, 1 sine, 2 constant
     float T0, Tf, t0, tf, period;
+    float T_first;     // temperature of the first update (T0 unless the caller set another)
     unsigned long long seed;
     int nbx, nby, nbz, brick_base;
     int pot;           // PotKind

@@ -45,9 +45,10 @@ __device__ __forceinline__ float temp_protocol(const SysDev &S, float t) {
 }
 // Temperature seen by the update of reference step ni: temp_set was last set
 // after the update of step ni-1 with time = dt * (1 + (float)(ni-1))
-// (main.cu:520-524); the first step of a run uses T0 (main.cu:156).
+// (main.cu:520-524); the first step of a run uses the temp_set the run
+// starts with: T0 (main.cu:156), or the caller's T_first.
 __device__ __forceinline__ float step_temperature(const SysDev &S, long long ni, long long ni_first) {
-    if (ni == ni_first) return S.T0;
+    if (ni == ni_first) return S.T_first;
     float t = __double2float_rn(__dmul_rn(S.dt_d, __dadd_rn(1.0, (double)(float)(ni - 1))));
     return temp_protocol(S, t);
 }
@@ -137,7 +138,8 @@ __global__ void k_order_keys(const float *__restrict__ pos3, int P, const int *_
         const int iz = min(max((int)__fmul_rn(z, S.cinv), 0), nc - 1);
         const int b = ix / bx + S.nbx * (iy / by + S.nby * (iz / bz));
         const int c = ix % bx + bx * (iy % by + by * (iz % bz));
-        const int slot = (S.brick_base + b) * V + c;
+        const int sp = (g - S.part_base) < S.n_big ? 0 : 1;
+        const int slot = ((S.brick_base + b) * 2 + sp) * V + c;  // brick, species, cell
         slot_of[g] = slot;
         atomicAdd(slot_cnt + slot, 1);
     }

@@ -12,7 +12,7 @@
 // raises a device flag; the rebuild kernels of the next step run only when the
 // flag is set (they exit at once otherwise), so CUDA graphs need no host
 // decision.  (Conditional graph nodes around the rebuild kernels, switched on
-// by the step kernel, measured 2% slower than these four early exits.)
+// by the step kernel, measured 2% slower than these early exits.)
 //
 // State by storage id: pos[2][P + 1] float4 (double-buffered: x, y, z and
 // w = storage id | species << 31; entry P is the zero position that list
@@ -33,16 +33,17 @@ constexpr int kMaxNbr = 64;
 #endif
 constexpr int kGather = BD_LIST_GATHER;
 // Launch variants of the list step, chosen per engine by the autotuner:
-// CTA size, resident CTAs per SM asked of the register allocator (8 x 128
-// threads: 64 registers; 9 x 128: 56), and whether the particle's own state
-// (remainder, build position, reference index) is loaded before the force
-// loop (its latency hidden under the gathers) or after it (fewer registers
-// live in the loop).  Each particle's arithmetic is the same in every
-// variant, so results do not depend on the choice.
+// CTA size, resident CTAs per SM asked of the register allocator (9 x 128
+// threads: 56 registers; 8 x 128: 64), and whether the particle's own state
+// (remainder, build position, reference index) is loaded after the force
+// loop (fewer registers live in the loop, so more warps hide the gathers)
+// or before it (its latency hidden under the gathers).  Each particle's
+// arithmetic is the same in every variant, so results do not depend on the
+// choice.  Variant 0, the default, measured fastest on the aging workload.
 template <int V> struct ListVariant;
-template <> struct ListVariant<0> { static constexpr int kThreads = 128, kMinBlocks = 8; static constexpr bool kLate = false; };
-template <> struct ListVariant<1> { static constexpr int kThreads = 256, kMinBlocks = 4; static constexpr bool kLate = false; };
-template <> struct ListVariant<2> { static constexpr int kThreads = 128, kMinBlocks = 9; static constexpr bool kLate = true; };
+template <> struct ListVariant<0> { static constexpr int kThreads = 128, kMinBlocks = 9; static constexpr bool kLate = true; };
+template <> struct ListVariant<1> { static constexpr int kThreads = 128, kMinBlocks = 8; static constexpr bool kLate = false; };
+template <> struct ListVariant<2> { static constexpr int kThreads = 256, kMinBlocks = 4; static constexpr bool kLate = false; };
 constexpr int kListVariants = 3;
 constexpr int kListBuildThreads = 256;  // CTA size of the list build
 static_assert(kGather % 2 == 0 && kMaxNbr % kGather == 0, "partners are paired for f32x2 arithmetic");
@@ -189,8 +190,10 @@ struct ListBuild {
     int *nnb;
     float4 *pbuild;
     const float4 *pos_sid;
-    const int *flag;  // [R + 1] as in ListArgs
+    int *flag;                // [R + 1] as in ListArgs; cleared by the build's last block
     int nrep;
+    long long *builds;        // [0] replica list builds, [1] steps that rebuilt
+    unsigned *blocks_done;    // blocks of this launch that have finished (reset by the last one)
 };
 
 // Lists of every home particle of each brick (grid-stride over bricks):
@@ -273,21 +276,29 @@ __global__ void __launch_bounds__(kListBuildThreads, 2) k_list_build(StepArgs a,
         }
         __syncthreads();  // the next brick reuses the staging memory
     }
-}
-
-// clear the flags after a rebuild; builds[0] counts replica rebuilds,
-// builds[1] the steps that rebuilt
-__global__ void k_list_done(int *flag, int nrep, long long *builds) {
-    if (flag[nrep] == 0) return;
-    if (threadIdx.x == 0) atomicAdd((unsigned long long *)(builds + 1), 1ull);
+    // The last block to finish clears the flags, every block having read
+    // them (one launch per step fewer than a separate clearing kernel);
+    // builds[0] counts replica rebuilds, builds[1] the steps that rebuilt.
+    __shared__ bool last;
+    if (tid == 0) {
+        __threadfence();
+        last = atomicAdd(lb.blocks_done, 1u) == gridDim.x - 1;
+    }
     __syncthreads();
-    for (int r = threadIdx.x; r < nrep; r += blockDim.x)
-        if (flag[r]) {
-            atomicAdd((unsigned long long *)builds, 1ull);
-            flag[r] = 0;
+    if (last) {
+        __threadfence();
+        if (tid == 0) atomicAdd((unsigned long long *)(lb.builds + 1), 1ull);
+        for (int r = tid; r < nrep; r += T)
+            if (lb.flag[r]) {
+                atomicAdd((unsigned long long *)lb.builds, 1ull);
+                lb.flag[r] = 0;
+            }
+        __syncthreads();
+        if (tid == 0) {
+            lb.flag[nrep] = 0;
+            *lb.blocks_done = 0;
         }
-    __syncthreads();
-    if (threadIdx.x == 0) flag[nrep] = 0;
+    }
 }
 
 // ------------------------------------------------------------- step

@@ -53,7 +53,8 @@ class SystemDesc(C.Structure):
                 ("sigma_sml", C.c_float), ("mob_big", C.c_float), ("mob_sml", C.c_float), ("dt", C.c_double),
                 ("temp_protocol", C.c_int), ("T0", C.c_float), ("Tf", C.c_float), ("t0", C.c_float),
                 ("tf", C.c_float), ("period", C.c_float), ("seed", C.c_ulonglong), ("force_cap", C.c_float),
-                ("potential", C.c_int), ("pot_param", C.c_float * 4)]
+                ("potential", C.c_int), ("pot_param", C.c_float * 4), ("first_temp_set", C.c_int),
+                ("T_first", C.c_float)]
 
 
 class EngineOpts(C.Structure):
@@ -345,6 +346,7 @@ class System:
     force_cap: float = 0.0
     potential: str = "wca_modified"  # POTENTIAL keys; parameters in pot_param (bd_aging.h BD_POT_*)
     pot_param: tuple = (0.0, 0.0, 0.0, 0.0)
+    T_first: float = None  # temperature of the first update (None: T0)
 
     def desc(self) -> SystemDesc:
         d = SystemDesc()
@@ -363,6 +365,8 @@ class System:
         d.potential = POTENTIAL[self.potential]
         for k in range(4):
             d.pot_param[k] = float(self.pot_param[k]) if k < len(self.pot_param) else 0.0
+        if self.T_first is not None:
+            d.first_temp_set, d.T_first = 1, float(self.T_first)
         return d
 
     @property

@@ -246,6 +246,11 @@ typedef struct bd_system_desc {
     float force_cap;           /* > 0: |F| capped (initial-configuration relaxation) */
     int potential;             /* BD_POT_* (0: the reference's modified WCA) */
     float pot_param[4];        /* parameters of the potential, see BD_POT_* */
+    int first_temp_set;        /* != 0: the replica's first update runs at T_first instead of T0.
+                                  The reference sets temp_set to T0 once, before its loop over
+                                  configurations (main.cu:156), so every configuration after the
+                                  first starts at the temperature the previous one ended on */
+    float T_first;
 } bd_system_desc;
 
 /* Pair potentials (potentials.cu).  The reference's step uses the modified

@@ -6,7 +6,7 @@ the reference's generators are not in its repository, run-fself.sh:84-86):
   oracle.c:or_eng_cap_forces, the engine update with the engine's Philox
   noise), in the neighbour-list step and in the 27-cell sweep;
 * make() relaxes uniform random placements into states where no pair is
-  closer than 0.75 of its WCA diameter (from under 0.05 before), written in
+  closer than 0.75 of its WCA diameter (from under 0.2 before), written in
   the reference's init_config format (main.cu:231-241, 377-394);
 * the reference's own executable (oracle/_ref, built from its sources) reads
   those files and runs on them."""
@@ -80,7 +80,7 @@ def test_make_configs_removes_overlaps_and_reference_reads_them(tmp_path):
     nb = ns = 500
     side0 = float(np.float32(CF.side_from_phi(nb, ns, 0.5)))
     start = CF.uniform_config(nb, ns, side0, 104729)  # make(seed=1)'s placement of configuration 1
-    assert min_pair_ratio(start, nb, side0) < 0.05  # random placement: deep overlaps
+    assert min_pair_ratio(start, nb, side0) < 0.2  # random placement: deep overlaps
     side, pos = MC.make(nb, ns, 0.5, 2, seed=1, relax_steps=2000)
     assert side == side0 and pos.shape == (2, 1000, 3)
     for k in range(2):
