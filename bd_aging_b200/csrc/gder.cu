@@ -21,6 +21,18 @@
 // (kGrBrick + 2m cells per axis) must not wrap onto itself, so every cell
 // appears at most once.
 //
+// Pair loop: a warp holds 32 home particles in registers and walks a quarter
+// of the staged candidates, all lanes reading the same candidate (a
+// shared-memory broadcast).  A candidate cell that the region reaches across
+// a face of the box carries the periodic shift s = L k (k = -1, 0, 1 per
+// axis) of its image next to the brick, and the difference is taken as
+// (x_i - x_j) - s, both roundings the reference's minimum image makes
+// (d - L floor(d / L + 1/2), get_gder.cu:113-115) when its floor equals k.
+// For a pair within range that is always the case: a separation below the
+// range is below L / 2, so the region's image of the cell is the minimum
+// image; and a pair whose minimum image lies within range has its cell in
+// the region at that image.  Pairs out of range are not counted either way.
+//
 // The bound assumes every particle lies in its cell to within
 // kGrTol * cell side.  The engine's wrap keeps positions in [0, L], but a
 // blown-up state can leave a coordinate outside the box by the rounding of
@@ -36,6 +48,7 @@ constexpr int kGrTileCells = 96;
 constexpr int kGrMaxCap = 24;
 constexpr int kGrHomeMax = kGrBrick * kGrBrick * kGrBrick * kGrMaxCap;
 constexpr int kGrTileMax = kGrTileCells * kGrMaxCap;
+constexpr int kGrQuarters = 4;  // candidate slices per warp task
 constexpr double kGrTol = 1e-3;  // allowed stick-out of a particle from its cell, in cell sides
 
 struct GrArgs {
@@ -96,20 +109,73 @@ __device__ int gr_scan(int *a, int n, int *wsum) {
 }
 
 // last index c in [0, n) with start[c] <= t
-// one unordered pair (i, j) within range: both ordered counts
-__device__ __forceinline__ void gr_count_pair(float4 pi, float4 pj, float side, float side_inv, const float *thr,
-                                              float inv_bin_size, int nbins, unsigned *hist) {
-    const float dx = min_image_gder_fast(__fsub_rn(pi.x, pj.x), side, side_inv);
-    const float dy = min_image_gder_fast(__fsub_rn(pi.y, pj.y), side, side_inv);
-    const float dz = min_image_gder_fast(__fsub_rn(pi.z, pj.z), side, side_inv);
-    const int bin = gr_bin_thr(dist2_rn(dx, dy, dz), thr, inv_bin_size, nbins);
-    if (bin >= 0) {
-        const unsigned ti = __float_as_uint(pi.w) >> 31, tj = __float_as_uint(pj.w) >> 31;
-        if (ti == tj) {
-            atomicAdd(&hist[3 * ti * nbins + bin], 2u);
-        } else {
-            atomicAdd(&hist[(2 * ti + tj) * nbins + bin], 1u);
-            atomicAdd(&hist[(2 * tj + ti) * nbins + bin], 1u);
+// one unordered pair (i, j), j at periodic shift s of its stored position:
+// both ordered counts when the pair is within range (range2_hi = the
+// smallest squared distance at or beyond the range, thr[nbins + 1])
+__device__ __forceinline__ void gr_count_shifted(float4 pi, float4 pj, float4 s, float range2_hi, const float *thr,
+                                                 float inv_bin_size, int nbins, unsigned *hist) {
+    const float dx = __fsub_rn(__fsub_rn(pi.x, pj.x), s.x);
+    const float dy = __fsub_rn(__fsub_rn(pi.y, pj.y), s.y);
+    const float dz = __fsub_rn(__fsub_rn(pi.z, pj.z), s.z);
+    const float d2 = dist2_rn(dx, dy, dz);
+    if (!(d2 < range2_hi)) return;
+    int b = (int)fmaxf(0.f, __fmul_rn(__fmul_rn(d2, rsqrtf(d2)), inv_bin_size));
+    b = min(b, nbins);
+    if (b < nbins && d2 >= thr[b + 1]) b++;
+    else if (b > 0 && d2 < thr[b]) b--;
+    const int bin = min(b, nbins - 1);
+    const unsigned ti = __float_as_uint(pi.w) >> 31, tj = __float_as_uint(pj.w) >> 31;
+    if (ti == tj) {
+        atomicAdd(&hist[3 * ti * nbins + bin], 2u);
+    } else {
+        atomicAdd(&hist[(2 * ti + tj) * nbins + bin], 1u);
+        atomicAdd(&hist[(2 * tj + ti) * nbins + bin], 1u);
+    }
+}
+
+__device__ __forceinline__ int gr_find(const int *start, int n, int t);
+
+// Warp tasks over (32 home particles) x (a quarter of the candidates
+// cand[0, nc)): the lanes keep their home particle in registers and read
+// each candidate together.  HOME: the candidates are the home particles
+// themselves and a pair counts once (smaller storage id first); otherwise
+// the candidates of tile cell k are cand[start[k], start[k + 1]) and carry
+// the cell's periodic shift cshift[k] (the cell index advances with the
+// candidate index, the same in every lane).
+template <bool HOME>
+__device__ __forceinline__ void gr_warp_tasks(const float4 *home, int H, const float4 *cand, const int *start,
+                                              const float4 *cshift, int ncells, int nc, float range2_hi,
+                                              const float *thr, float inv_bin_size, int nbins, unsigned *hist) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int groups = (H + 31) >> 5;
+    const int per = (nc + kGrQuarters - 1) / kGrQuarters;
+    for (int task = warp; task < groups * kGrQuarters; task += nwarps) {
+        const int g = task / kGrQuarters, q = task % kGrQuarters;
+        const int h = (g << 5) + lane;
+        const bool live = h < H;
+        const float4 pi = home[live ? h : 0];
+        const unsigned si = __float_as_uint(pi.w) & 0x7fffffffu;
+        const int c0 = q * per, c1 = min(nc, (q + 1) * per);
+        if (c0 >= c1) continue;
+        int cell = 0, cend = nc;
+        float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (!HOME) {
+            cell = gr_find(start, ncells, c0);
+            cend = start[cell + 1];
+            s = cshift[cell];
+        }
+        for (int c = c0; c < c1; c++) {
+            if (!HOME && c >= cend) {  // next non-empty cell (uniform over the warp)
+                do { cell++; cend = start[cell + 1]; } while (c >= cend);
+                s = cshift[cell];
+            }
+            const float4 pj = cand[c];
+            if (HOME) {
+                if (live && si < (__float_as_uint(pj.w) & 0x7fffffffu))
+                    gr_count_shifted(pi, pj, s, range2_hi, thr, inv_bin_size, nbins, hist);
+            } else if (live) {
+                gr_count_shifted(pi, pj, s, range2_hi, thr, inv_bin_size, nbins, hist);
+            }
         }
     }
 }
@@ -129,6 +195,7 @@ __global__ void __launch_bounds__(kGrThreads) k_gr_cells(GrArgs a) {
     float4 *tile = home + kGrHomeMax;
     int *cstart = reinterpret_cast<int *>(tile + kGrTileMax);  // [kGrTileCells + 1]
     int *cgc = cstart + kGrTileCells + 1;                       // [kGrTileCells]
+    __shared__ float4 cshift[kGrTileCells];                     // periodic shift of each tile cell
     int *wsum = cgc + kGrTileCells;                             // [kGrThreads / 32 + 1]
     unsigned *hist = reinterpret_cast<unsigned *>(wsum + kGrThreads / 32 + 4);  // [4][nbins]
     float *thr = reinterpret_cast<float *>(hist + 4 * a.nbins);                   // [nbins + 2]
@@ -140,7 +207,6 @@ __global__ void __launch_bounds__(kGrThreads) k_gr_cells(GrArgs a) {
     const int wx = min(kGrBrick, nc - ox), wy = min(kGrBrick, nc - oy), wz = min(kGrBrick, nc - oz);
     const int nbins = a.nbins;
     const float side = S.L;
-    const float side_inv = __double2float_rn(1.0 / (double)side);
     const float range = a.range;
     const float inv_bin_size = 1.0f / __fdiv_rn(range, (float)nbins);  // estimate only (gr_bin_thr)
     // cells whose nearest point is farther than range: gap g (cells) with
@@ -181,28 +247,17 @@ __global__ void __launch_bounds__(kGrThreads) k_gr_cells(GrArgs a) {
         return;
     }
 
+    const float range2_hi = thr[nbins + 1];  // thr was filled before the home staging barriers
     if (H > 0) {
-        // 2. pairs inside the home brick, each once (smaller storage id first)
-        {
-            const int nhh = H * H;
-            int h = tid % H, c = tid / H;
-            const int dh = kGrThreads % H, dc = kGrThreads / H;
-            for (int p = tid; p < nhh; p += kGrThreads) {
-                const float4 pi = home[h], pj = home[c];
-                if ((__float_as_uint(pi.w) & 0x7fffffffu) < (__float_as_uint(pj.w) & 0x7fffffffu))
-                    gr_count_pair(pi, pj, side, side_inv, thr, inv_bin_size, nbins, hist);
-                h += dh;
-                c += dc;
-                if (h >= H) { h -= H; c++; }
-            }
-        }
+        // 2. pairs inside the home brick, each once (smaller storage id
+        // first); the brick does not wrap, so no shift
+        gr_warp_tasks<true>(home, H, home, nullptr, nullptr, 0, H, range2_hi, thr, inv_bin_size, nbins, hist);
         // 3. candidate region, tile by tile: only cells of bricks after the
         // home brick (brick order of the grid this kernel tiles with)
         const int nbr = (nc + kGrBrick - 1) / kGrBrick;
         const int hb = ox / kGrBrick + nbr * (oy / kGrBrick + nbr * (oz / kGrBrick));
         const int rx = wx + 2 * m, ry = wy + 2 * m, rz = wz + 2 * m;
         const int nreg = rx * ry * rz;
-        const int dh = kGrThreads % H, dc = kGrThreads / H;
         for (int c0 = 0; c0 < nreg; c0 += kGrTileCells) {
             const int ntc = min(kGrTileCells, nreg - c0);
             for (int q = tid; q < ntc; q += kGrThreads) {
@@ -215,6 +270,12 @@ __global__ void __launch_bounds__(kGrThreads) k_gr_cells(GrArgs a) {
                 int k = 0, gc = 0;
                 if ((float)(kx * kx + ky * ky + kz * kz) <= lim2) {
                     int gx = ox - m + lx, gy = oy - m + ly, gz = oz - m + lz;
+                    // a cell reached across a face: its image next to the
+                    // brick is the stored position minus L (k = -1) or plus L
+                    const float sx = gx < 0 ? -side : (gx >= nc ? side : 0.f);
+                    const float sy = gy < 0 ? -side : (gy >= nc ? side : 0.f);
+                    const float sz = gz < 0 ? -side : (gz >= nc ? side : 0.f);
+                    cshift[q] = make_float4(sx, sy, sz, 0.f);
                     gx += gx < 0 ? nc : 0; gx -= gx >= nc ? nc : 0;
                     gy += gy < 0 ? nc : 0; gy -= gy >= nc ? nc : 0;
                     gz += gz < 0 ? nc : 0; gz -= gz >= nc ? nc : 0;
@@ -234,15 +295,8 @@ __global__ void __launch_bounds__(kGrThreads) k_gr_cells(GrArgs a) {
                 tile[t] = a.pos[(size_t)cgc[c] * a.cap + (t - cstart[c])];
             }
             __syncthreads();
-            // pairs (home h, candidate c) of different bricks, h fastest
-            const int np = H * Tn;
-            int h = tid % H, c = tid / H;
-            for (int p = tid; p < np; p += kGrThreads) {
-                gr_count_pair(home[h], tile[c], side, side_inv, thr, inv_bin_size, nbins, hist);
-                h += dh;
-                c += dc;
-                if (h >= H) { h -= H; c++; }
-            }
+            // pairs (home h, candidate c) of different bricks
+            gr_warp_tasks<false>(home, H, tile, cstart, cshift, ntc, Tn, range2_hi, thr, inv_bin_size, nbins, hist);
             __syncthreads();
         }
     }
