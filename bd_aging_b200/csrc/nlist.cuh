@@ -336,6 +336,7 @@ __device__ __forceinline__ void list_forces_wca(const ListArgs &a, int sid, int 
                                                 float sg0, float sg1, float c0, float c1, float &fx, float &fy,
                                                 float &fz) {
     const f2 PX = f2_bcast(pi.x), PY = f2_bcast(pi.y), PZ = f2_bcast(pi.z), M12 = f2_bcast(-12.0f);
+    const float sq0 = sg0 * sg0, sq1 = sg1 * sg1;
     f2 FX = 0ull, FY = 0ull, FZ = 0ull;  // (0.f, 0.f)
     const int np = a.np;
     int jn[kGather];
@@ -370,12 +371,16 @@ __device__ __forceinline__ void list_forces_wca(const ListArgs &a, int sid, int 
             const bool oka = (!WRAP || jj[u] != np) && d2a < (ta ? c1 : c0);
             const bool okb = (!WRAP || jj[u + 1] != np) && d2b < (tb ? c1 : c0);
             if (oka || okb) {
-                const f2 DI = f2_make(rsqrtf(d2a), rsqrtf(d2b));
-                const f2 SOR = f2_mul(DI, f2_make(ta ? sg1 : sg0, tb ? sg1 : sg0));
-                const f2 S2 = f2_mul(SOR, SOR);
+                // (s / r)^2 from one approximate reciprocal of r^2 (one
+                // multiply pair fewer than from 1 / r)
+                float ra, rb;
+                asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(ra) : "f"(d2a));
+                asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rb) : "f"(d2b));
+                const f2 R2 = f2_make(ra, rb);
+                const f2 S2 = f2_mul(R2, f2_make(ta ? sq1 : sq0, tb ? sq1 : sq0));
                 const f2 S6 = f2_mul(f2_mul(S2, S2), S2);
                 // -12 (s^12 - s^6) / r^2
-                const f2 G = f2_mul(f2_mul(M12, f2_sub(f2_mul(S6, S6), S6)), f2_mul(DI, DI));
+                const f2 G = f2_mul(f2_mul(M12, f2_sub(f2_mul(S6, S6), S6)), R2);
                 float ga, gb;
                 f2_split(G, ga, gb);
                 const f2 GM = f2_make(oka ? ga : 0.f, okb ? gb : 0.f);

@@ -336,7 +336,8 @@ int bd_engine_get_positions(bd_engine *e, float *pos_host, float *raw_host);
 /* g(r) counts of the current state: counts_host[nsys][4][nbins] (bb, bs, sb,
  * ss ordered pairs, get_gder.cu arithmetic), exact integers. */
 int bd_engine_gder(bd_engine *e, int nbins, float range, unsigned long long *counts_host);
-#define BD_GDER_AUTO 0       /* per replica: cell-bounded when the range is small against the box */
+#define BD_GDER_AUTO 0       /* per replica: cell-bounded whenever the box holds the stencil region
+                                (4 + 2 ceil(range / cell side) cells per axis), else all pairs */
 #define BD_GDER_ALL_PAIRS 1  /* every pair, as get_gder_dev (get_gder.cu:69-127) */
 #define BD_GDER_CELLS 2      /* only cells within the range (BD_ERR_ARG if a replica's box
                                 is under 4 + 2 ceil(range / cell side) cells) */
