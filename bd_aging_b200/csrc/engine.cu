@@ -577,6 +577,10 @@ int setup_geometry(bd_engine *e) {
         S.interior = rcmax + 2.0f * skin + 0.01f;
         int nc = (int)std::floor((double)d.side / ((double)(rcmax + skin) * (1.0 + 1e-5)));
         if (nc < 3) return BD_ERR_ARG;  // box too small for a 27-cell sweep
+        // the list step's minimum image (min_image_pair) needs every list
+        // partner well within L / 2 of the particle: with skin at most 0.9 of
+        // the largest cut distance and three cells per side, within 0.492 L
+        if (e->list && skin > 0.9f * rcmax) return BD_ERR_ARG;
         S.ncell = nc;
         S.cinv = (float)nc / d.side;
         S.cell_base = (int)cell_base;

@@ -324,6 +324,21 @@ __device__ __forceinline__ void gather_chunk(const ListArgs &a, const int (&jn)[
     }
 }
 
+// The reference's minimum image d - L floor(d / L + 1/2) (get_forces.cu)
+// of two list partners at once.  A list partner lies within cut + 2 skin of
+// the particle, and a box holds at least three cells of side cut + skin with
+// skin at most 0.9 of the largest cut (checked at engine creation), so d / L
+// is within 0.492 of an integer k: then
+// floor(d / L + 1/2) = rint(d / L) = k, L k is exact, and one rounded
+// fma(k, -L, d) is the reference's rounded difference.  (A pair whose
+// quotient lay near a half integer would sit near L / 2, beyond every cut
+// distance, and fail the cut test with either rounding.)
+__device__ __forceinline__ f2 min_image_pair(f2 d, f2 linv, f2 neg_l) {
+    float ta, tb;
+    f2_split(f2_mul(d, linv), ta, tb);
+    return f2_fma(f2_make(rintf(ta), rintf(tb)), neg_l, d);
+}
+
 // Modified-WCA force on one particle from its list, two partners per f32x2
 // operation (each lane rounds as the scalar operation does).  WRAP: a
 // partner may lie across the periodic boundary, so each displacement takes
@@ -337,6 +352,7 @@ __device__ __forceinline__ void list_forces_wca(const ListArgs &a, int sid, int 
                                                 float &fz) {
     const f2 PX = f2_bcast(pi.x), PY = f2_bcast(pi.y), PZ = f2_bcast(pi.z), M12 = f2_bcast(-12.0f);
     const float sq0 = sg0 * sg0, sq1 = sg1 * sg1;
+    const f2 LINV = f2_bcast(Linv), NEGL = f2_bcast(-L);
     f2 FX = 0ull, FY = 0ull, FZ = 0ull;  // (0.f, 0.f)
     const int np = a.np;
     int jn[kGather];
@@ -353,13 +369,9 @@ __device__ __forceinline__ void list_forces_wca(const ListArgs &a, int sid, int 
             f2 dY = f2_sub(f2_make(qa.y, qb.y), PY);
             f2 dZ = f2_sub(f2_make(qa.z, qb.z), PZ);
             if (WRAP) {
-                float xa, xb, ya, yb, za, zb;
-                f2_split(dX, xa, xb);
-                f2_split(dY, ya, yb);
-                f2_split(dZ, za, zb);
-                dX = f2_make(min_image_fast(xa, L, Linv), min_image_fast(xb, L, Linv));
-                dY = f2_make(min_image_fast(ya, L, Linv), min_image_fast(yb, L, Linv));
-                dZ = f2_make(min_image_fast(za, L, Linv), min_image_fast(zb, L, Linv));
+                dX = min_image_pair(dX, LINV, NEGL);
+                dY = min_image_pair(dY, LINV, NEGL);
+                dZ = min_image_pair(dZ, LINV, NEGL);
             }
             // dist2_rn in each lane
             const f2 D2 = f2_add(f2_add(f2_mul(dX, dX), f2_mul(dY, dY)), f2_mul(dZ, dZ));

@@ -284,7 +284,9 @@ typedef struct bd_engine_opts {
     float neighbor_skin;       /* > 0 (default 0.25): neighbour-list mode (plain mode,
                                   generated noise): lists of partners within cut + skin,
                                   rebuilt on the device when a particle of the replica
-                                  has moved skin / 2; 0: the 27-cell sweep every step */
+                                  has moved skin / 2; 0: the 27-cell sweep every step.
+                                  At most 1, and at most 0.9 of each replica's largest
+                                  cut distance (BD_ERR_ARG otherwise) */
     int list_variant;          /* list-step launch variant 0 .. BD_LIST_VARIANTS-1 (CTA size,
                                   registers, load placement; same results), or -1 (default):
                                   variant 0, or with autotune chosen with the brick shape
