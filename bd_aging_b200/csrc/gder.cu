@@ -124,13 +124,11 @@ __device__ __forceinline__ void gr_count_shifted(float4 pi, float4 pj, float4 s,
     if (b < nbins && d2 >= thr[b + 1]) b++;
     else if (b > 0 && d2 < thr[b]) b--;
     const int bin = min(b, nbins - 1);
+    // species pair bb 0, bs 1, ss 2: an equal-species pair adds its two
+    // ordered counts to one bin; a mixed pair one count to bs and one to sb
+    // at the same bin, so bs and sb are one histogram (copied at the end)
     const unsigned ti = __float_as_uint(pi.w) >> 31, tj = __float_as_uint(pj.w) >> 31;
-    if (ti == tj) {
-        atomicAdd(&hist[3 * ti * nbins + bin], 2u);
-    } else {
-        atomicAdd(&hist[(2 * ti + tj) * nbins + bin], 1u);
-        atomicAdd(&hist[(2 * tj + ti) * nbins + bin], 1u);
-    }
+    atomicAdd(&hist[(ti + tj) * nbins + bin], ti == tj ? 2u : 1u);
 }
 
 __device__ __forceinline__ int gr_find(const int *start, int n, int t);
@@ -198,7 +196,7 @@ __global__ void __launch_bounds__(kGrThreads) k_gr_cells(GrArgs a) {
     __shared__ float4 cshift[kGrTileCells];                     // periodic shift of each tile cell
     int *wsum = cgc + kGrTileCells;                             // [kGrThreads / 32 + 1]
     unsigned *hist = reinterpret_cast<unsigned *>(wsum + kGrThreads / 32 + 4);  // [4][nbins]
-    float *thr = reinterpret_cast<float *>(hist + 4 * a.nbins);                   // [nbins + 2]
+    float *thr = reinterpret_cast<float *>(hist + 3 * a.nbins);                   // [nbins + 2]
     const int tid = threadIdx.x;
     const int4 br = a.bricks[blockIdx.x];
     const SysDev &S = a.sys[br.x];
@@ -215,7 +213,7 @@ __global__ void __launch_bounds__(kGrThreads) k_gr_cells(GrArgs a) {
     const float tol = (float)kGrTol * cs;
     const float lim = (range / cs) * 1.00001f + 4.0f * (float)kGrTol;
     const float lim2 = lim * lim;
-    for (int b = tid; b < 4 * nbins; b += kGrThreads) hist[b] = 0;
+    for (int b = tid; b < 3 * nbins; b += kGrThreads) hist[b] = 0;
     for (int b = tid; b < nbins + 2; b += kGrThreads) thr[b] = a.thr[b];
 
     // 1. home particles of the brick
@@ -301,9 +299,13 @@ __global__ void __launch_bounds__(kGrThreads) k_gr_cells(GrArgs a) {
         }
     }
     __syncthreads();
-    unsigned long long *out = a.counts + (size_t)br.x * 4 * nbins;
-    for (int b = tid; b < 4 * nbins; b += kGrThreads)
-        if (hist[b]) atomicAdd(&out[b], (unsigned long long)hist[b]);
+    unsigned long long *out = a.counts + (size_t)br.x * 4 * nbins;  // bb, bs, sb, ss
+    for (int b = tid; b < 3 * nbins; b += kGrThreads) {
+        const unsigned v = hist[b];
+        if (!v) continue;
+        atomicAdd(&out[b < 2 * nbins ? b : b + nbins], (unsigned long long)v);  // bb, bs / ss
+        if (b >= nbins && b < 2 * nbins) atomicAdd(&out[b + nbins], (unsigned long long)v);  // sb = bs
+    }
 }
 
 // Stencil reach of replica r for `range`, or -1 when the candidate region
@@ -319,7 +321,7 @@ int gder_cell_reach(const SysDev &S, float range) {
 
 size_t gder_cells_smem(int nbins) {
     return sizeof(float4) * (kGrHomeMax + kGrTileMax) + sizeof(int) * (2 * kGrTileCells + 1 + kGrThreads / 32 + 4) +
-           sizeof(unsigned) * 4 * (size_t)nbins + sizeof(float) * (nbins + 2);
+           sizeof(unsigned) * 3 * (size_t)nbins + sizeof(float) * (nbins + 2);
 }
 
 // Counts of the replicas with m_of[r] >= 0 into d_counts.  A replica whose

@@ -549,10 +549,13 @@ __global__ void __launch_bounds__(ListVariant<V>::kThreads, ListVariant<V>::kMin
     a.lo_z[sid] = lz;
     if (!(isfinite(x) && isfinite(y) && isfinite(z))) set_status(a.status, kStatNumeric);
     a.pos_out[sid] = make_float4(x, y, z, pi.w);
-    // skin check against the positions at the last build
-    const float bx = min_image_fast(__fsub_rn(x, pb.x), L, Linv);
-    const float by = min_image_fast(__fsub_rn(y, pb.y), L, Linv);
-    const float bz = min_image_fast(__fsub_rn(z, pb.z), L, Linv);
+    // skin check against the positions at the last build: the minimum image
+    // as in min_image_pair (a displacement near L / 2 raises the flag with
+    // either rounding of the image)
+    const float dbx = __fsub_rn(x, pb.x), dby = __fsub_rn(y, pb.y), dbz = __fsub_rn(z, pb.z);
+    const float bx = fmaf(rintf(__fmul_rn(Linv, dbx)), -L, dbx);
+    const float by = fmaf(rintf(__fmul_rn(Linv, dby)), -L, dby);
+    const float bz = fmaf(rintf(__fmul_rn(Linv, dbz)), -L, dbz);
     if (!(dist2_rn(bx, by, bz) <= S.skin_half2)) {
         a.flag[a.rep_of_sid[sid]] = 1;
         a.flag[a.nrep] = 1;
