@@ -259,9 +259,10 @@ def reference_cuda(steps=200):
 
 def gder_leg(eng, systems, nbins=400, rng=15.0, iters=3):
     """g(r) counts of every replica (bd_engine_gder, exact integers; the
-    reference scripts' 400 bins to r = 15, run-fself.sh:46-47).  Work =
-    ordered pairs tested: N^2 per replica on the all-pairs path, or the
-    candidates of the cell stencil."""
+    reference scripts' 400 bins to r = 15, run-fself.sh:46-47), by the
+    engine's choice of method (the cell stencil wherever the box holds its
+    region, else all pairs).  Rate: the N (N - 1) ordered pairs of each
+    replica that the reference's all-pairs kernel tests, per second."""
     import torch
     eng.gder(nbins, rng)
     st = torch.cuda.ExternalStream(eng.stream_handle())
@@ -271,8 +272,9 @@ def gder_leg(eng, systems, nbins=400, rng=15.0, iters=3):
     st.synchronize()
     t = (time.perf_counter() - t0) / iters
     pairs = float(sum(s.n * (s.n - 1) for s in systems))
-    return {"ms_per_call": t * 1e3, "nbins": nbins, "range": rng, "ordered_pairs": pairs,
-            "pair_evaluations_per_s": pairs / t, "note": "wall time of the call (exact u64 counts copied back)"}
+    return {"ms_per_call": t * 1e3, "nbins": nbins, "range": rng, "method": "auto", "ordered_pairs": pairs,
+            "all_pairs_equivalent_per_s": pairs / t,
+            "note": "wall time of the call (exact u64 counts copied back)"}
 
 
 def correlator_leg(eng, P, slots=16, iters=20, q=6.19):
