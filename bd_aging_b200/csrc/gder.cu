@@ -133,29 +133,17 @@ __device__ __forceinline__ void gr_count_shifted(float4 pi, float4 pj, float4 s,
 
 __device__ __forceinline__ int gr_find(const int *start, int n, int t);
 
-// squared gap between the box [lo, hi] and the cell [c, c + w] on each axis
-__device__ __forceinline__ float gr_gap2(float3 lo, float3 hi, float4 c, float w) {
-    const float gx = fmaxf(0.f, fmaxf(c.x - hi.x, lo.x - (c.x + w)));
-    const float gy = fmaxf(0.f, fmaxf(c.y - hi.y, lo.y - (c.y + w)));
-    const float gz = fmaxf(0.f, fmaxf(c.z - hi.z, lo.z - (c.z + w)));
-    return gx * gx + gy * gy + gz * gz;
-}
-
 // Warp tasks over (32 home particles) x (a quarter of the candidates
 // cand[0, nc)): the lanes keep their home particle in registers and read
 // each candidate together.  HOME: the candidates are the home particles
 // themselves and a pair counts once (smaller storage id first); otherwise
 // the candidates of tile cell k are cand[start[k], start[k + 1]) and carry
 // the cell's periodic shift cshift[k] (the cell index advances with the
-// candidate index, the same in every lane), and a cell whose image box
-// (corner cbox[k], side cw, both already widened by the particles' allowed
-// stick-out) lies farther than the range from the bounding box of the warp's
-// home particles is skipped whole: no pair of it can count.
+// candidate index, the same in every lane).
 template <bool HOME>
 __device__ __forceinline__ void gr_warp_tasks(const float4 *home, int H, const float4 *cand, const int *start,
-                                              const float4 *cshift, const float4 *cbox, float cw, float skip2,
-                                              int ncells, int nc, float range2_hi, const float *thr,
-                                              float inv_bin_size, int nbins, unsigned *hist) {
+                                              const float4 *cshift, int ncells, int nc, float range2_hi,
+                                              const float *thr, float inv_bin_size, int nbins, unsigned *hist) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const int groups = (H + 31) >> 5;
     const int per = (nc + kGrQuarters - 1) / kGrQuarters;
@@ -163,36 +151,23 @@ __device__ __forceinline__ void gr_warp_tasks(const float4 *home, int H, const f
         const int g = task / kGrQuarters, q = task % kGrQuarters;
         const int h = (g << 5) + lane;
         const bool live = h < H;
-        const float4 pi = home[live ? h : (g << 5)];  // a dead lane repeats the group's first particle
+        const float4 pi = home[live ? h : 0];
         const unsigned si = __float_as_uint(pi.w) & 0x7fffffffu;
         const int c0 = q * per, c1 = min(nc, (q + 1) * per);
         if (c0 >= c1) continue;
         int cell = 0, cend = nc;
         float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
-        float3 lo = make_float3(pi.x, pi.y, pi.z), hi = lo;
         if (!HOME) {
-#pragma unroll
-            for (int o = 16; o; o >>= 1) {
-                lo.x = fminf(lo.x, __shfl_xor_sync(0xffffffffu, lo.x, o));
-                lo.y = fminf(lo.y, __shfl_xor_sync(0xffffffffu, lo.y, o));
-                lo.z = fminf(lo.z, __shfl_xor_sync(0xffffffffu, lo.z, o));
-                hi.x = fmaxf(hi.x, __shfl_xor_sync(0xffffffffu, hi.x, o));
-                hi.y = fmaxf(hi.y, __shfl_xor_sync(0xffffffffu, hi.y, o));
-                hi.z = fmaxf(hi.z, __shfl_xor_sync(0xffffffffu, hi.z, o));
-            }
-            cell = gr_find(start, ncells, c0) - 1;
-            cend = c0;  // the loop enters the first cell and tests it
+            cell = gr_find(start, ncells, c0);
+            cend = start[cell + 1];
+            s = cshift[cell];
         }
-        for (int c = c0; c < c1;) {
+        for (int c = c0; c < c1; c++) {
             if (!HOME && c >= cend) {  // next non-empty cell (uniform over the warp)
                 do { cell++; cend = start[cell + 1]; } while (c >= cend);
                 s = cshift[cell];
-                if (gr_gap2(lo, hi, cbox[cell], cw) > skip2) {  // no pair of this cell within range
-                    c = cend;
-                    continue;
-                }
             }
-            const float4 pj = cand[c++];
+            const float4 pj = cand[c];
             if (HOME) {
                 if (live && si < (__float_as_uint(pj.w) & 0x7fffffffu))
                     gr_count_shifted(pi, pj, s, range2_hi, thr, inv_bin_size, nbins, hist);
@@ -219,7 +194,6 @@ __global__ void __launch_bounds__(kGrThreads) k_gr_cells(GrArgs a) {
     int *cstart = reinterpret_cast<int *>(tile + kGrTileMax);  // [kGrTileCells + 1]
     int *cgc = cstart + kGrTileCells + 1;                       // [kGrTileCells]
     __shared__ float4 cshift[kGrTileCells];                     // periodic shift of each tile cell
-    __shared__ float4 cbox[kGrTileCells];                       // corner of its image next to the brick
     int *wsum = cgc + kGrTileCells;                             // [kGrThreads / 32 + 1]
     unsigned *hist = reinterpret_cast<unsigned *>(wsum + kGrThreads / 32 + 4);  // [4][nbins]
     float *thr = reinterpret_cast<float *>(hist + 3 * a.nbins);                   // [nbins + 2]
@@ -272,17 +246,10 @@ __global__ void __launch_bounds__(kGrThreads) k_gr_cells(GrArgs a) {
     }
 
     const float range2_hi = thr[nbins + 1];  // thr was filled before the home staging barriers
-    // a cell is skipped when its image box, widened on every side by the
-    // stick-out tol its particles may have (home positions are exact), is
-    // farther than the range plus a relative margin that covers the float
-    // arithmetic of the gap and of the images (cs * nc against L)
-    const float skip_d = range * 1.0001f;
-    const float skip2 = skip_d * skip_d;
     if (H > 0) {
         // 2. pairs inside the home brick, each once (smaller storage id
         // first); the brick does not wrap, so no shift
-        gr_warp_tasks<true>(home, H, home, nullptr, nullptr, nullptr, 0.f, 0.f, 0, H, range2_hi, thr, inv_bin_size,
-                            nbins, hist);
+        gr_warp_tasks<true>(home, H, home, nullptr, nullptr, 0, H, range2_hi, thr, inv_bin_size, nbins, hist);
         // 3. candidate region, tile by tile: only cells of bricks after the
         // home brick (brick order of the grid this kernel tiles with)
         const int nbr = (nc + kGrBrick - 1) / kGrBrick;
@@ -307,8 +274,6 @@ __global__ void __launch_bounds__(kGrThreads) k_gr_cells(GrArgs a) {
                     const float sy = gy < 0 ? -side : (gy >= nc ? side : 0.f);
                     const float sz = gz < 0 ? -side : (gz >= nc ? side : 0.f);
                     cshift[q] = make_float4(sx, sy, sz, 0.f);
-                    // widened by the stick-out tol on every side
-                    cbox[q] = make_float4((float)gx * cs - tol, (float)gy * cs - tol, (float)gz * cs - tol, 0.f);
                     gx += gx < 0 ? nc : 0; gx -= gx >= nc ? nc : 0;
                     gy += gy < 0 ? nc : 0; gy -= gy >= nc ? nc : 0;
                     gz += gz < 0 ? nc : 0; gz -= gz >= nc ? nc : 0;
@@ -329,8 +294,7 @@ __global__ void __launch_bounds__(kGrThreads) k_gr_cells(GrArgs a) {
             }
             __syncthreads();
             // pairs (home h, candidate c) of different bricks
-            gr_warp_tasks<false>(home, H, tile, cstart, cshift, cbox, cs + 2.f * tol, skip2, ntc, Tn, range2_hi, thr,
-                                 inv_bin_size, nbins, hist);
+            gr_warp_tasks<false>(home, H, tile, cstart, cshift, ntc, Tn, range2_hi, thr, inv_bin_size, nbins, hist);
             __syncthreads();
         }
     }
