@@ -521,11 +521,12 @@ def run_ours(args):
     achieved = ALG_BYTES_PER_PARTICLE_STEP * P / avg_launch_s / 1e9
     list_mode = info.neighbor_skin > 0
     tpp = profile_traffic_per_particle_step(list_mode)
-    # kernels per time step: the list step plus its four rebuild kernels (which
-    # exit at once when no list is stale), or the one sweep kernel; per
-    # 96-step graph the counter kernel, plus the noise-amplitude table in list
-    # mode (persistent mode: the persistent kernel and the counter)
-    per_step = 5 if list_mode else (1 if args.mode == "plain" else 0)
+    # kernels per time step: the list step plus its three rebuild kernels
+    # (clear, bin, build; they exit at once when no list is stale), or the one
+    # sweep kernel; per 96-step graph the counter kernel, plus the
+    # noise-amplitude table in list mode (persistent mode: the persistent
+    # kernel and the counter)
+    per_step = 4 if list_mode else (1 if args.mode == "plain" else 0)
     per_graph = 2 if (list_mode or not per_step) else 1
     gpu_launches = args.steps * (math.ceil(S / 96) * per_graph + per_step * S)
     line = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
