@@ -16,9 +16,10 @@
 //
 // State by storage id: pos[2][P + 1] float4 (double-buffered: x, y, z and
 // w = storage id | species << 31; entry P is the zero position that list
-// padding gathers), positions at the last build, the lists [kMaxNbr][P]
-// (slot-major: the threads of a warp read consecutive words, padded to whole
-// gather chunks), list lengths, the compensated remainder shared with the
+// padding gathers), positions at the last build, the lists
+// [kMaxNbr / 4][P][4] (chunks of four words per particle: a thread reads a
+// gather chunk in one load, the threads of a warp consecutive chunks; padded
+// to whole chunks), list lengths, the compensated remainder shared with the
 // sweep path, and face crossings per axis [3][P] in place of a per-step FP64
 // displacement (k_list_dsp rebuilds it for observations).  Cell buckets
 // (cnt / pos of buffer 0) are rebuilt from the by-id positions for list
@@ -47,6 +48,13 @@ template <> struct ListVariant<2> { static constexpr int kThreads = 256, kMinBlo
 constexpr int kListVariants = 3;
 constexpr int kListBuildThreads = 256;  // CTA size of the list build
 static_assert(kGather % 2 == 0 && kMaxNbr % kGather == 0, "partners are paired for f32x2 arithmetic");
+static_assert(kGather == 4, "the list words of a gather chunk are one int4");
+// Word k of particle sid's list.  Lists are stored in chunks of four words
+// per particle, [k / 4][sid][k % 4]: a gather chunk is one 16-byte load per
+// thread, consecutive threads reading consecutive chunks.
+__device__ __forceinline__ size_t list_slot(int k, int sid, int np) {
+    return ((size_t)(k >> 2) * np + sid) * 4 + (k & 3);
+}
 
 struct ListArgs {
     const SysDev *sys;
@@ -57,7 +65,7 @@ struct ListArgs {
     float4 *pos_out;        // by storage id, next step
     float *lo_x, *lo_y, *lo_z;
     int *img;               // [3][np]: box lengths crossed per axis since the origin
-    const int *nbr;         // [kMaxNbr][np]
+    const int *nbr;         // [kMaxNbr / 4][np][4] (list_slot)
     const int *nnb;         // [np]
     const float *amp_tab;   // [step in launch batch][R][species] noise amplitudes (k_amp_table)
     const float4 *pbuild;   // positions at the last build
@@ -242,7 +250,7 @@ __global__ void __launch_bounds__(kListBuildThreads, 2) k_list_build(StepArgs a,
                 auto flush = [&]() {
                     for (int e = 0; e < nq; e++) {
                         if (cnt < kMaxNbr) {
-                            if (ok_sid) lb.nbr[(size_t)cnt * a.np + home_sid] = sm.ssid[sm.queue[e * T + tid]];
+                            if (ok_sid) lb.nbr[list_slot(cnt, home_sid, a.np)] = sm.ssid[sm.queue[e * T + tid]];
                         } else {
                             set_status(a.status, kStatCellOverflow);
                         }
@@ -266,7 +274,7 @@ __global__ void __launch_bounds__(kListBuildThreads, 2) k_list_build(StepArgs a,
                 if (ok_sid) {
                     const int nl = min(cnt, kMaxNbr);
                     // pad to whole gather chunks with storage id np (the zero position)
-                    for (int k = nl; k < kMaxNbr && (k % kGather) != 0; k++) lb.nbr[(size_t)k * a.np + home_sid] = a.np;
+                    for (int k = nl; k < kMaxNbr && (k % kGather) != 0; k++) lb.nbr[list_slot(k, home_sid, a.np)] = a.np;
                     lb.nnb[home_sid] = nl;
                     lb.pbuild[home_sid] = lb.pos_sid[home_sid];
                 } else {
@@ -311,7 +319,11 @@ __global__ void __launch_bounds__(kListBuildThreads, 2) k_list_build(StepArgs a,
 // list words k0 .. k0 + kGather - 1 (k0 < kMaxNbr)
 __device__ __forceinline__ void list_words(const ListArgs &a, int sid, int k0, int (&jn)[kGather]) {
 #pragma unroll
-    for (int u = 0; u < kGather; u++) jn[u] = __ldg(a.nbr + (size_t)(k0 + u) * a.np + sid);
+    const int4 w = __ldg(reinterpret_cast<const int4 *>(a.nbr) + (size_t)(k0 >> 2) * a.np + sid);
+    jn[0] = w.x;
+    jn[1] = w.y;
+    jn[2] = w.z;
+    jn[3] = w.w;
 }
 // positions of the chunk's partners: an entry outside [0, np) reads the zero
 // position at np and counts as absent (jj = np)
@@ -611,7 +623,7 @@ __global__ void k_census_list(ListArgs a, double *obs) {
     unsigned long long h = 0;
     const int n = min(a.nnb[sid], kMaxNbr);
     for (int k = 0; k < n; k++) {
-        const int j = a.nbr[(size_t)k * a.np + sid];
+        const int j = a.nbr[list_slot(k, sid, a.np)];
         if ((unsigned)j >= (unsigned)a.np) continue;
         const float4 pj = a.pos_in[j];
         const float dx = min_image_fast(__fsub_rn(pj.x, pi.x), L, Linv);
