@@ -348,6 +348,32 @@ int launch_list_step(bd_engine *e, const ListArgs &a, int ni_off) {
             }
     }
 }
+// Launch variants 3-5: one block per replica runs `nsteps` steps (the
+// Philox noise only; other noise streams take variant 0).
+bool list_per_replica(const bd_engine *e) {
+    return e->list && e->lvar >= kListFirstPersistent && e->rng == BD_RNG_PHILOX;
+}
+template <int V>
+int launch_list_replica_v(bd_engine *e, int cur, int nsteps) {
+    constexpr int T = ListVariant<V>::kThreads;
+    const ListArgs a = make_largs(e, cur);
+    const ListPersist lp{{e->lpos[0], e->lpos[1]}, cur & 1, e->cnt[0], e->pos[0], e->cap, e->nbr, e->nnb,
+                         e->pbuild, e->d_rep_order, e->d_builds, e->d_step_rebuilt};
+    if (e->extra_pot) k_list_replica<true, V><<<e->R, T, 0, e->stream>>>(a, lp, e->d_ni, nsteps);
+    else k_list_replica<false, V><<<e->R, T, 0, e->stream>>>(a, lp, e->d_ni, nsteps);
+    BD_LAUNCH_CHECK();
+    k_list_replica_done<<<1, 256, 0, e->stream>>>(e->lflag, e->R, e->d_step_rebuilt, nsteps, e->d_builds);
+    BD_LAUNCH_CHECK();
+    return BD_OK;
+}
+int list_replica_steps(bd_engine *e, int cur, int nsteps) {
+    if (nsteps > e->graph_steps) return BD_ERR_ARG;  // the amplitude table holds one batch
+    switch (e->lvar) {
+        case 3: return launch_list_replica_v<3>(e, cur, nsteps);
+        case 4: return launch_list_replica_v<4>(e, cur, nsteps);
+        default: return launch_list_replica_v<5>(e, cur, nsteps);
+    }
+}
 // one list-mode step in phase `cur`: gated rebuild, then the step
 int list_step(bd_engine *e, int cur, int ni_off) {
     int rc = list_rebuild(e, cur);
@@ -389,9 +415,13 @@ int direct_steps(bd_engine *e, int k) {
     if (e->list) {
         if (k > e->graph_steps) return BD_ERR_ARG;  // the amplitude table holds one batch
         if (int rc = list_amplitudes(e, k)) return rc;
-        for (int i = 0; i < k; i++) {
-            int rc = list_step(e, e->cur + i, i);
-            if (rc) return rc;
+        if (list_per_replica(e)) {
+            if (int rc = list_replica_steps(e, e->cur, k)) return rc;
+        } else {
+            for (int i = 0; i < k; i++) {
+                int rc = list_step(e, e->cur + i, i);
+                if (rc) return rc;
+            }
         }
         k_advance_counter<<<1, 1, 0, e->stream>>>(e->d_ni, k);
         BD_LAUNCH_CHECK();
@@ -418,7 +448,9 @@ int build_graph(bd_engine *e) {
     int rc = BD_OK;
     if (e->list) {
         rc = list_amplitudes(e, e->graph_steps);
-        for (int j = 0; j < e->graph_steps && rc == BD_OK; j++) rc = list_step(e, e->cur + j, j);
+        if (rc == BD_OK && list_per_replica(e)) rc = list_replica_steps(e, e->cur, e->graph_steps);
+        else
+            for (int j = 0; j < e->graph_steps && rc == BD_OK; j++) rc = list_step(e, e->cur + j, j);
     } else if (e->mode == BD_MODE_PERSISTENT) {
         StepArgs a = make_args(e, e->cur, 1);
         rc = launch_persistent(e, a, e->graph_steps);
@@ -446,7 +478,8 @@ void free_engine(bd_engine *e) {
                     e->status, e->d_ni, e->out_pos, e->out_raw, e->d_cl_start, e->d_cl_bricks, e->rn_ring, e->rn_lcg,
                     e->snaps, e->d_segs, e->d_seg_first, e->corr_part, e->corr_out, e->lpos[0], e->lpos[1],
                     e->pbuild, e->nbr, e->nnb, e->lflag, e->d_one, e->d_builds, e->ld_in, e->ld_staged,
-                    e->ld_slot, e->ld_bucket, e->ld_cnt, e->ld_start, e->ld_bsum, e->ld_bad, e->img, e->amp_tab};
+                    e->ld_slot, e->ld_bucket, e->ld_cnt, e->ld_start, e->ld_bsum, e->ld_bad, e->img, e->amp_tab,
+                    e->d_rep_order, e->d_step_rebuilt};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -723,6 +756,17 @@ int bd_engine_create(const bd_system_desc *systems, int nsys, const bd_engine_op
         ALLOC(e->d_one, sizeof(int));
         ALLOC(e->d_builds, 3 * sizeof(long long));  // + the build's finished-block counter
         cudaMemsetAsync(e->d_builds, 0, 3 * sizeof(long long), e->stream);
+        ALLOC(e->d_step_rebuilt, sizeof(int) * e->graph_steps);
+        cudaMemsetAsync(e->d_step_rebuilt, 0, sizeof(int) * e->graph_steps, e->stream);
+        ALLOC(e->d_rep_order, sizeof(int) * e->R);
+        {  // blocks of a per-replica launch start with the largest replicas
+            std::vector<int> order(e->R);
+            std::iota(order.begin(), order.end(), 0);
+            std::stable_sort(order.begin(), order.end(),
+                             [&](int a, int b) { return e->sysh[a].n > e->sysh[b].n; });
+            cudaMemcpyAsync(e->d_rep_order, order.data(), sizeof(int) * e->R, cudaMemcpyHostToDevice, e->stream);
+            cudaStreamSynchronize(e->stream);  // the host vector goes out of scope
+        }
         const int one = 1;
         cudaMemcpyAsync(e->d_one, &one, sizeof(int), cudaMemcpyHostToDevice, e->stream);
     }
@@ -904,9 +948,14 @@ int autotune_list(bd_engine *e, long long &nsteps) {
     static const int shapes[][3] = {{4, 4, 3}, {4, 4, 4}, {3, 3, 3}, {5, 4, 4}, {4, 4, 2}};
     struct Cand { int bx, by, bz, v; };
     std::vector<Cand> cands;
-    for (auto &sh : shapes)
-        for (int v = 0; v < kListVariants; v++)
-            if (e->tune_lvar || v == e->lvar) cands.push_back({sh[0], sh[1], sh[2], v});
+    for (int v = 0; v < kListVariants; v++) {
+        if (!(e->tune_lvar || v == e->lvar)) continue;
+        if (v >= kListFirstPersistent) {  // builds its lists in the block: no brick shape to choose
+            if (e->rng == BD_RNG_PHILOX) cands.push_back({e->bx, e->by, e->bz, v});
+            continue;
+        }
+        for (auto &sh : shapes) cands.push_back({sh[0], sh[1], sh[2], v});
+    }
     const int warm = 2, timed = 12;
     if (nsteps < (long long)cands.size() * (warm + timed) + 1) return BD_OK;  // too short to tune now
     cudaEvent_t t0, t1;

@@ -82,6 +82,8 @@ struct bd_engine {
     long long *d_builds = nullptr;  // [0] replica list builds, [1] steps that rebuilt
     int *img = nullptr;             // [3][P] face crossings since the origin (displacement on demand)
     float *amp_tab = nullptr;       // [graph_steps][R][2] noise amplitudes of a launch batch
+    int *d_rep_order = nullptr;     // per-replica launch (variants 3-5): replica of each block
+    int *d_step_rebuilt = nullptr;  // [graph_steps] steps of such a launch that rebuilt a replica
     // set_positions scratch (storage order computed on the device)
     float *ld_in = nullptr;        // [P][3] positions as given
     float4 *ld_staged = nullptr;   // [P] in storage order

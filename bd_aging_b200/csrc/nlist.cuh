@@ -45,7 +45,12 @@ template <int V> struct ListVariant;
 template <> struct ListVariant<0> { static constexpr int kThreads = 128, kMinBlocks = 9; static constexpr bool kLate = true; };
 template <> struct ListVariant<1> { static constexpr int kThreads = 128, kMinBlocks = 8; static constexpr bool kLate = false; };
 template <> struct ListVariant<2> { static constexpr int kThreads = 256, kMinBlocks = 4; static constexpr bool kLate = false; };
-constexpr int kListVariants = 3;
+// 3-5: one block per replica running a whole batch of steps (k_list_replica)
+template <> struct ListVariant<3> { static constexpr int kThreads = 256, kMinBlocks = 4; static constexpr bool kLate = true; };
+template <> struct ListVariant<4> { static constexpr int kThreads = 512, kMinBlocks = 2; static constexpr bool kLate = true; };
+template <> struct ListVariant<5> { static constexpr int kThreads = 1024, kMinBlocks = 1; static constexpr bool kLate = true; };
+constexpr int kListVariants = 6;
+constexpr int kListFirstPersistent = 3;
 constexpr int kListBuildThreads = 256;  // CTA size of the list build
 static_assert(kGather % 2 == 0 && kMaxNbr % kGather == 0, "partners are paired for f32x2 arithmetic");
 static_assert(kGather == 4, "the list words of a gather chunk are one int4");
@@ -316,10 +321,20 @@ __global__ void __launch_bounds__(kListBuildThreads, 2) k_list_build(StepArgs a,
 // padded to whole chunks with storage id np, whose position entry is zero and
 // never written, so a chunk needs no per-entry length test.
 
+// Loads of the list state: through the read-only path in the per-step
+// kernels (NC), plain loads in the per-replica persistent kernel, which
+// rewrites positions and lists during its launch (a block sees its own
+// writes after a barrier; the read-only path gives no such guarantee).
+template <bool NC, typename T>
+__device__ __forceinline__ T ld_state(const T *p) {
+    if constexpr (NC) return __ldg(p);
+    else return *p;
+}
+
 // list words k0 .. k0 + kGather - 1 (k0 < kMaxNbr)
+template <bool NC = true>
 __device__ __forceinline__ void list_words(const ListArgs &a, int sid, int k0, int (&jn)[kGather]) {
-#pragma unroll
-    const int4 w = __ldg(reinterpret_cast<const int4 *>(a.nbr) + (size_t)(k0 >> 2) * a.np + sid);
+    const int4 w = ld_state<NC>(reinterpret_cast<const int4 *>(a.nbr) + (size_t)(k0 >> 2) * a.np + sid);
     jn[0] = w.x;
     jn[1] = w.y;
     jn[2] = w.z;
@@ -327,12 +342,13 @@ __device__ __forceinline__ void list_words(const ListArgs &a, int sid, int k0, i
 }
 // positions of the chunk's partners: an entry outside [0, np) reads the zero
 // position at np and counts as absent (jj = np)
+template <bool NC = true>
 __device__ __forceinline__ void gather_chunk(const ListArgs &a, const int (&jn)[kGather], int (&jj)[kGather],
                                              float4 (&pj)[kGather]) {
 #pragma unroll
     for (int u = 0; u < kGather; u++) {
         jj[u] = (int)min((unsigned)jn[u], (unsigned)a.np);
-        pj[u] = __ldg(a.pos_in + jj[u]);
+        pj[u] = ld_state<NC>(a.pos_in + jj[u]);
     }
 }
 
@@ -358,7 +374,7 @@ __device__ __forceinline__ f2 min_image_pair(f2 d, f2 linv, f2 neg_l) {
 // around the particle and the minimum image would return the plain
 // difference.  The force is summed in two interleaved partial sums (even and
 // odd list positions) that are added at the end.
-template <bool WRAP>
+template <bool WRAP, bool NC = true>
 __device__ __forceinline__ void list_forces_wca(const ListArgs &a, int sid, int n, float4 pi, float L, float Linv,
                                                 float sg0, float sg1, float c0, float c1, float &fx, float &fy,
                                                 float &fz) {
@@ -368,12 +384,12 @@ __device__ __forceinline__ void list_forces_wca(const ListArgs &a, int sid, int 
     f2 FX = 0ull, FY = 0ull, FZ = 0ull;  // (0.f, 0.f)
     const int np = a.np;
     int jn[kGather];
-    if (n > 0) list_words(a, sid, 0, jn);
+    if (n > 0) list_words<NC>(a, sid, 0, jn);
     for (int k0 = 0; k0 < n; k0 += kGather) {
         int jj[kGather];
         float4 pj[kGather];
-        gather_chunk(a, jn, jj, pj);
-        if (k0 + kGather < n) list_words(a, sid, k0 + kGather, jn);
+        gather_chunk<NC>(a, jn, jj, pj);
+        if (k0 + kGather < n) list_words<NC>(a, sid, k0 + kGather, jn);
 #pragma unroll
         for (int u = 0; u < kGather; u += 2) {
             const float4 qa = pj[u], qb = pj[u + 1];
@@ -425,6 +441,7 @@ __device__ __forceinline__ void list_forces_wca(const ListArgs &a, int sid, int 
 
 // Force from the list for a replica with another potential of PotKind
 // (scalar, list order).
+template <bool NC = true>
 __device__ __forceinline__ void list_forces_extra(const ListArgs &a, const SysDev &S, int sid, int n, float4 pi, int tm,
                                                float &fx, float &fy, float &fz) {
     const float L = S.L, Linv = S.Linv;
@@ -432,12 +449,12 @@ __device__ __forceinline__ void list_forces_extra(const ListArgs &a, const SysDe
     const float c0 = tm ? S.cut2[1] : S.cut2[0], c1 = tm ? S.cut2[2] : S.cut2[1];
     fx = fy = fz = 0.f;
     int jn[kGather];
-    if (n > 0) list_words(a, sid, 0, jn);
+    if (n > 0) list_words<NC>(a, sid, 0, jn);
     for (int k0 = 0; k0 < n; k0 += kGather) {
         int jj[kGather];
         float4 pj[kGather];
-        gather_chunk(a, jn, jj, pj);
-        if (k0 + kGather < n) list_words(a, sid, k0 + kGather, jn);
+        gather_chunk<NC>(a, jn, jj, pj);
+        if (k0 + kGather < n) list_words<NC>(a, sid, k0 + kGather, jn);
 #pragma unroll
         for (int u = 0; u < kGather; u++) {
             if (jj[u] == a.np) continue;
@@ -459,18 +476,16 @@ __device__ __forceinline__ void list_forces_extra(const ListArgs &a, const SysDe
     }
 }
 
-// One time step of every particle from its list (thread per storage id).
-// Force sum in list order; update, compensated position and FP64
-// displacement exactly as process_brick.
+// One time step of particle sid from its list: force sum in list order;
+// update, compensated position and FP64 displacement exactly as
+// process_brick.  Returns true when the particle has moved more than half
+// the skin since the last build (its replica's lists must be rebuilt).
 // EXTRA: some replica of the batch uses a potential other than the modified
 // WCA (instantiated separately so the default kernel keeps its registers).
-template <int RNG, bool EXTRA, int V>
-__global__ void __launch_bounds__(ListVariant<V>::kThreads, ListVariant<V>::kMinBlocks)
-    k_step_list(ListArgs a, const long long *ni_base, int ni_off) {
-    const int sid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (sid >= a.np) return;
-    const long long ni = *ni_base + ni_off;
-    const int rep = a.rep_of_sid[sid];
+// LATE: the particle's own state is loaded after the force loop.  NC: loads
+// through the read-only path (ld_state).
+template <int RNG, bool EXTRA, bool LATE, bool NC>
+__device__ __forceinline__ bool list_particle_step(const ListArgs &a, int sid, int rep, long long ni, int ni_off) {
     const SysDev &S = a.sys[rep];
     const float L = S.L, Linv = S.Linv;
     const float4 pi = a.pos_in[sid];
@@ -481,15 +496,15 @@ __global__ void __launch_bounds__(ListVariant<V>::kThreads, ListVariant<V>::kMin
     int gid;
     float lx, ly, lz;
     float4 pb;
-    if constexpr (!ListVariant<V>::kLate) {  // own state early: its latency overlaps the force loop
+    if constexpr (!LATE) {  // own state early: its latency overlaps the force loop
         gid = __ldg(a.gid_of + sid);
         lx = a.lo_x[sid], ly = a.lo_y[sid], lz = a.lo_z[sid];
-        pb = __ldg(a.pbuild + sid);
+        pb = ld_state<NC>(a.pbuild + sid);
     }
     float fx, fy, fz;
-    const int n = min(__ldg(a.nnb + sid), kMaxNbr);
+    const int n = min(ld_state<NC>(a.nnb + sid), kMaxNbr);
     if (EXTRA && S.pot != kPotWcaModified) {
-        list_forces_extra(a, S, sid, n, pi, tm, fx, fy, fz);
+        list_forces_extra<NC>(a, S, sid, n, pi, tm, fx, fy, fz);
     } else {  // the same arithmetic in either instantiation: a replica's result does not depend on its batch
         // a warp whose particles all sit away from the faces needs no
         // minimum image for any partner
@@ -497,9 +512,9 @@ __global__ void __launch_bounds__(ListVariant<V>::kThreads, ListVariant<V>::kMin
         const bool inner = pi.x >= lo_edge && pi.x <= hi_edge && pi.y >= lo_edge && pi.y <= hi_edge &&
                            pi.z >= lo_edge && pi.z <= hi_edge;
         if (__all_sync(__activemask(), inner))
-            list_forces_wca<false>(a, sid, n, pi, L, Linv, sg0, sg1, c0, c1, fx, fy, fz);
+            list_forces_wca<false, NC>(a, sid, n, pi, L, Linv, sg0, sg1, c0, c1, fx, fy, fz);
         else
-            list_forces_wca<true>(a, sid, n, pi, L, Linv, sg0, sg1, c0, c1, fx, fy, fz);
+            list_forces_wca<true, NC>(a, sid, n, pi, L, Linv, sg0, sg1, c0, c1, fx, fy, fz);
     }
     if (S.fcap > 0.f) {  // capped forces for the initial relaxation
         const float fmx = fmaxf(fabsf(fx), fmaxf(fabsf(fy), fabsf(fz)));
@@ -514,10 +529,10 @@ __global__ void __launch_bounds__(ListVariant<V>::kThreads, ListVariant<V>::kMin
             fx = fy = fz = 0.f;
         }
     }
-    if constexpr (ListVariant<V>::kLate) {
+    if constexpr (LATE) {
         gid = __ldg(a.gid_of + sid);
         lx = a.lo_x[sid], ly = a.lo_y[sid], lz = a.lo_z[sid];
-        pb = __ldg(a.pbuild + sid);
+        pb = ld_state<NC>(a.pbuild + sid);
     }
     const int pid = gid - S.part_base;
     if (ni == 0) {  // origin of the unwrapped positions (main.cu:497-506)
@@ -568,9 +583,193 @@ __global__ void __launch_bounds__(ListVariant<V>::kThreads, ListVariant<V>::kMin
     const float bx = fmaf(rintf(__fmul_rn(Linv, dbx)), -L, dbx);
     const float by = fmaf(rintf(__fmul_rn(Linv, dby)), -L, dby);
     const float bz = fmaf(rintf(__fmul_rn(Linv, dbz)), -L, dbz);
-    if (!(dist2_rn(bx, by, bz) <= S.skin_half2)) {
-        a.flag[a.rep_of_sid[sid]] = 1;
+    return !(dist2_rn(bx, by, bz) <= S.skin_half2);
+}
+
+// One time step of every particle (thread per storage id); a particle beyond
+// half the skin flags its replica for a rebuild before the next step.
+template <int RNG, bool EXTRA, int V>
+__global__ void __launch_bounds__(ListVariant<V>::kThreads, ListVariant<V>::kMinBlocks)
+    k_step_list(ListArgs a, const long long *ni_base, int ni_off) {
+    const int sid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sid >= a.np) return;
+    const int rep = a.rep_of_sid[sid];
+    if (list_particle_step<RNG, EXTRA, ListVariant<V>::kLate, true>(a, sid, rep, *ni_base + ni_off, ni_off)) {
+        a.flag[rep] = 1;
         a.flag[a.nrep] = 1;
+    }
+}
+
+// ------------------------------------------------------------- per-replica persistent launch
+// Launch variants 3-5 run a whole batch of steps in one launch, one block
+// per replica: the block steps its replica's particles, decides at a block
+// barrier whether any of them left half the skin, and if so rebuilds the
+// replica's cell buckets and lists itself before the next step.  Replicas
+// never interact, so blocks never wait on one another; a block's own writes
+// (positions, buckets, lists) are visible to its threads after each barrier,
+// which is why these kernels read the list state with plain loads.
+// The lists are the ones k_list_build writes: partners in the staged
+// sweep's order (rows dz, dy of three cells dx, each cell in storage-id
+// order), the same shifted differences and the same list cut test, so a
+// replica's trajectory does not depend on the variant.
+struct ListPersist {
+    float4 *pos[2];        // by-id positions, the two buffers
+    int cur0;              // buffer holding the input of the launch's first step
+    int *cnt;              // cell counts of the buckets (buffer 0)
+    float4 *bucket;        // [C][cap] cell buckets
+    int cap;
+    int *nbr;              // lists (list_slot), lengths and build positions:
+    int *nnb;              //   the writable views of ListArgs' nbr, nnb, pbuild
+    float4 *pbuild;
+    const int *order;      // replica of each block, most particles first
+    long long *builds;     // [0] replica list builds, [1] steps that rebuilt
+    int *step_rebuilt;     // [step of the launch]: some replica rebuilt before it
+};
+
+// cell of a by-id position, as bin_particle and the step kernels bin it
+__device__ __forceinline__ int3 list_cell_of(const float4 v, const SysDev &S) {
+    const int nc = S.ncell;
+    int ix = (int)__fmul_rn(v.x, S.cinv), iy = (int)__fmul_rn(v.y, S.cinv), iz = (int)__fmul_rn(v.z, S.cinv);
+    return make_int3(min(max(ix, 0), nc - 1), min(max(iy, 0), nc - 1), min(max(iz, 0), nc - 1));
+}
+// neighbour cell index along one axis (periodic) and the staged sweep's
+// shift of its particles (+L when the cell wrapped below 0, -L above nc - 1)
+__device__ __forceinline__ int wrap_cell(int g, int nc, float L, float &shift) {
+    int sgn = 0;
+    if (g < 0) { g += nc; sgn = 1; } else if (g >= nc) { g -= nc; sgn = -1; }
+    shift = __int2float_rn(sgn) * L;  // exact: sgn in {-1, 0, 1}
+    return g;
+}
+
+// List of particle sid from the sorted buckets of its replica.
+__device__ __forceinline__ void replica_list(const ListArgs &a, const ListPersist &lp, const SysDev &S, int sid) {
+    const float4 v = a.pos_in[sid];
+    const int np = a.np, nc = S.ncell, cap = lp.cap;
+    const int tm = (int)(__float_as_uint(v.w) >> 31);
+    const float cut_b = S.lcut2[tm], cut_s = S.lcut2[tm + 1];  // towards a big / a small partner
+    const float L = S.L;
+    const int3 c = list_cell_of(v, S);
+    int cnt = 0;
+    for (int dz = -1; dz <= 1; dz++) {
+        float shz;
+        const int gz = wrap_cell(c.z + dz, nc, L, shz);
+        for (int dy = -1; dy <= 1; dy++) {
+            float shy;
+            const int gy = wrap_cell(c.y + dy, nc, L, shy);
+            for (int dx = -1; dx <= 1; dx++) {
+                float shx;
+                const int gx = wrap_cell(c.x + dx, nc, L, shx);
+                const int gc = S.cell_base + gx + nc * (gy + nc * gz);
+                const int m = min(lp.cnt[gc], cap);
+                const float4 *b = lp.bucket + (size_t)gc * cap;
+                for (int k = 0; k < m; k++) {
+                    const float4 q = b[k];
+                    const unsigned wq = __float_as_uint(q.w);
+                    const int sj = (int)(wq & 0x7fffffffu);
+                    if (sj == sid) continue;
+                    const float ex = __fsub_rn(__fsub_rn(q.x, v.x), shx);
+                    const float ey = __fsub_rn(__fsub_rn(q.y, v.y), shy);
+                    const float ez = __fsub_rn(__fsub_rn(q.z, v.z), shz);
+                    if (dist2_rn(ex, ey, ez) < ((wq >> 31) ? cut_s : cut_b)) {
+                        if (cnt < kMaxNbr) lp.nbr[list_slot(cnt, sid, np)] = sj;
+                        else set_status(a.status, kStatCellOverflow);
+                        cnt++;
+                    }
+                }
+            }
+        }
+    }
+    const int nl = min(cnt, kMaxNbr);
+    for (int k = nl; k < kMaxNbr && (k % kGather) != 0; k++) lp.nbr[list_slot(k, sid, np)] = np;
+    lp.nnb[sid] = nl;
+    lp.pbuild[sid] = v;
+}
+
+// Buckets and lists of replica S from a.pos_in, by the whole block.
+__device__ __forceinline__ void replica_rebuild(const ListArgs &a, const ListPersist &lp, const SysDev &S) {
+    const int tid = threadIdx.x, T = blockDim.x;
+    const int nc = S.ncell, ncell = nc * nc * nc, cb = S.cell_base, cap = lp.cap;
+    const int base = S.part_base, end = S.part_base + S.n;
+    for (int c = tid; c < ncell; c += T) lp.cnt[cb + c] = 0;
+    __syncthreads();
+    for (int sid = base + tid; sid < end; sid += T) {
+        const float4 v = a.pos_in[sid];
+        const int3 c = list_cell_of(v, S);
+        const int cell = cb + c.x + nc * (c.y + nc * c.z);
+        const int slot = atomicAdd(lp.cnt + cell, 1);
+        if (slot < cap) lp.bucket[(size_t)cell * cap + slot] = v;
+        else set_status(a.status, kStatCellOverflow);
+    }
+    __syncthreads();
+    // each cell in storage-id order (insertion sort, a thread per cell)
+    for (int c = tid; c < ncell; c += T) {
+        float4 *b = lp.bucket + (size_t)(cb + c) * cap;
+        const int m = min(lp.cnt[cb + c], cap);
+        for (int i = 1; i < m; i++) {
+            const float4 v = b[i];
+            const unsigned key = __float_as_uint(v.w) & 0x7fffffffu;
+            int j = i - 1;
+            while (j >= 0 && (__float_as_uint(b[j].w) & 0x7fffffffu) > key) {
+                b[j + 1] = b[j];
+                j--;
+            }
+            b[j + 1] = v;
+        }
+    }
+    __syncthreads();
+    for (int sid = base + tid; sid < end; sid += T) replica_list(a, lp, S, sid);
+    __syncthreads();
+}
+
+// nsteps steps of replica order[blockIdx.x] (Philox noise; nsteps at most the
+// amplitude table's batch).  The replica's flag on entry asks for a rebuild
+// before the first step; on exit it holds the last step's verdict.
+template <bool EXTRA, int V>
+__global__ void __launch_bounds__(ListVariant<V>::kThreads, ListVariant<V>::kMinBlocks)
+    k_list_replica(ListArgs a, ListPersist lp, const long long *ni_base, int nsteps) {
+    const int rep = lp.order[blockIdx.x];
+    const SysDev &S = a.sys[rep];
+    const int base = S.part_base, end = S.part_base + S.n;
+    const long long ni0 = *ni_base;
+    bool need = a.flag[rep] != 0;
+    for (int s = 0; s < nsteps; s++) {
+        ListArgs as = a;
+        const bool odd = ((lp.cur0 + s) & 1) != 0;  // a select, not an indexed (local-memory) copy
+        as.pos_in = odd ? lp.pos[1] : lp.pos[0];
+        as.pos_out = odd ? lp.pos[0] : lp.pos[1];
+        if (need) {
+            replica_rebuild(as, lp, S);
+            if (threadIdx.x == 0) {
+                atomicAdd((unsigned long long *)lp.builds, 1ull);
+                lp.step_rebuilt[s] = 1;
+            }
+        }
+        bool beyond = false;
+        for (int sid = base + (int)threadIdx.x; sid < end; sid += blockDim.x)
+            beyond |= list_particle_step<kRngPhilox, EXTRA, ListVariant<V>::kLate, false>(as, sid, rep, ni0 + s, s);
+        need = __syncthreads_or(beyond) != 0;
+    }
+    if (threadIdx.x == 0) a.flag[rep] = need ? 1 : 0;
+}
+
+// After a per-replica launch: the any-replica flag from the per-replica
+// flags, and the launch's steps that rebuilt some replica counted.
+__global__ void k_list_replica_done(int *flag, int nrep, int *step_rebuilt, int nsteps, long long *builds) {
+    __shared__ int s_any, s_steps;
+    if (threadIdx.x == 0) s_any = s_steps = 0;
+    __syncthreads();
+    int any = 0, steps = 0;
+    for (int r = threadIdx.x; r < nrep; r += blockDim.x) any |= flag[r];
+    for (int s = threadIdx.x; s < nsteps; s += blockDim.x) {
+        steps += step_rebuilt[s] != 0;
+        step_rebuilt[s] = 0;
+    }
+    if (any) atomicOr(&s_any, 1);
+    if (steps) atomicAdd(&s_steps, steps);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        flag[nrep] = s_any;
+        if (s_steps) atomicAdd((unsigned long long *)(builds + 1), (unsigned long long)s_steps);
     }
 }
 

@@ -600,7 +600,7 @@ def run_ours(args):
         line["workloads"] = {}
         for wl in ("batched", "large", "small"):  # BASELINE configs 3, 4 and 1 beside the headline (config 2)
             try:
-                line["workloads"][wl] = workload_leg(wl, autotune=(wl == "batched"))
+                line["workloads"][wl] = workload_leg(wl, autotune=(wl in ("batched", "small")))
             except Exception as ex:  # reported, never fatal for the bench line
                 line["workloads"][wl] = {"error": str(ex)[:200]}
         line["precision"] = precision_leg()

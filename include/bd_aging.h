@@ -287,12 +287,16 @@ typedef struct bd_engine_opts {
                                   has moved skin / 2; 0: the 27-cell sweep every step.
                                   At most 1, and at most 0.9 of each replica's largest
                                   cut distance (BD_ERR_ARG otherwise) */
-    int list_variant;          /* list-step launch variant 0 .. BD_LIST_VARIANTS-1 (CTA size,
-                                  registers, load placement; same results), or -1 (default):
-                                  variant 0, or with autotune chosen with the brick shape
-                                  at the first run */
+    int list_variant;          /* list-step launch variant 0 .. BD_LIST_VARIANTS-1, same
+                                  results in every variant: 0-2 launch each step (CTA size,
+                                  registers, load placement) with separate rebuild kernels;
+                                  3-5 run a whole batch of steps in one launch, one block
+                                  of 256 / 512 / 1024 threads per replica that rebuilds its
+                                  replica's lists itself (Philox noise; the other noise
+                                  streams run variant 0).  -1 (default): variant 0, or with
+                                  autotune chosen with the brick shape at the first run */
 } bd_engine_opts;
-#define BD_LIST_VARIANTS 3
+#define BD_LIST_VARIANTS 6
 
 typedef struct bd_observables {
     double energy_big, energy_sml; /* (1/N) sum 0.5 pot_i per species (main.cu:627-631) */

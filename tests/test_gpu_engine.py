@@ -211,33 +211,44 @@ def test_autotuner_changes_speed_not_results():
 def test_list_autotuner_and_launch_variants_change_speed_not_results():
     """List mode: every list-step launch variant, and the autotuner's choice
     of variant and build brick (timed on the live batch), give the same bits
-    as the default layout."""
+    as the default layout.  Variants 3-5 run each batch of steps in one
+    launch, one block per replica that rebuilds its own lists: their
+    rebuild decisions (counted per replica and per step) and their lists
+    are those of the per-step kernels."""
     systems, poss = _ragged(4, 71)
     pos = np.concatenate(poss)
     ref = B.Engine(list(systems))
     assert ref.info().neighbor_skin > 0 and ref.info().list_variant == 0
     ref.set_positions(pos)
-    ref.run(400)
+    ref.run(400)  # four 96-step graphs and 16 single steps
     want = ref.get_positions()
-    for v in (1, 2):
+    ref_info = ref.info()
+    assert ref_info.list_builds > 4 and ref_info.list_rebuild_steps > 1
+    cnt_ref, hsh_ref = ref.census()
+    for v in (1, 2, 3, 4, 5):
         ev = B.Engine(list(systems), list_variant=v)
         assert ev.info().list_variant == v
         ev.set_positions(pos)
         ev.run(400)
         got = ev.get_positions()
-        np.testing.assert_array_equal(got[0], want[0])
-        np.testing.assert_array_equal(got[1], want[1])
+        np.testing.assert_array_equal(got[0], want[0], err_msg="variant %d" % v)
+        np.testing.assert_array_equal(got[1], want[1], err_msg="variant %d" % v)
+        info = ev.info()
+        assert (info.list_builds, info.list_rebuild_steps) == (ref_info.list_builds, ref_info.list_rebuild_steps), v
+        cnt, hsh = ev.census()
+        np.testing.assert_array_equal(cnt, cnt_ref)
+        np.testing.assert_array_equal(hsh, hsh_ref)
         ev.close()
     ea = B.Engine(list(systems), autotune=1)
     ea.set_positions(pos)
-    ea.run(400)  # 15 candidates x 14 steps are timed inside the first call
+    ea.run(400)  # 18 candidates x 14 steps are timed inside the first call
     info = ea.info()
-    assert info.tuned_ms > 0 and 0 <= info.list_variant < 3
+    assert info.tuned_ms > 0 and 0 <= info.list_variant < 6
     got = ea.get_positions()
     np.testing.assert_array_equal(got[0], want[0])
     np.testing.assert_array_equal(got[1], want[1])
     with pytest.raises(B.BDError):
-        B.Engine(list(systems), list_variant=3)
+        B.Engine(list(systems), list_variant=6)
 
 
 def test_first_step_temperature_carried_over():
