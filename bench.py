@@ -525,9 +525,11 @@ def run_ours(args):
     # (clear, bin, build; they exit at once when no list is stale), or the one
     # sweep kernel; per 96-step graph the counter kernel, plus the
     # noise-amplitude table in list mode (persistent mode: the persistent
-    # kernel and the counter)
-    per_step = 4 if list_mode else (1 if args.mode == "plain" else 0)
-    per_graph = 2 if (list_mode or not per_step) else 1
+    # kernel and the counter; per-replica list variants 3-5: the amplitude
+    # table, the per-replica kernel, its flag kernel and the counter)
+    per_replica = list_mode and info.list_variant >= 3
+    per_step = 0 if per_replica else (4 if list_mode else (1 if args.mode == "plain" else 0))
+    per_graph = 4 if per_replica else (2 if (list_mode or not per_step) else 1)
     gpu_launches = args.steps * (math.ceil(S / 96) * per_graph + per_step * S)
     line = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
