@@ -22,7 +22,10 @@
 // first call on each device (with that device current) looks the address up
 // with cudaGetSymbolAddress and caches it for that device's context; a device
 // reset, which destroys the context, makes the next call look it up again.
-// Make that first call on a device before any stream capture begins.
+// Make that first call on a device before a global-mode stream capture
+// starts anywhere in the process (the lookup is a runtime call such a
+// capture refuses).  The entry point synchronises its stream to read the sum
+// back, so it cannot itself be captured.
 #include <mutex>
 
 #include "runtime.cuh"

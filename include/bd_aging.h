@@ -170,10 +170,12 @@ int bd_fself_isotropic(const float *rr_raw, const float *rr0, int ngrain, float 
  * memory is reserved up front by another allocator.  Its scratch is a fixed
  * 32 KB device array per GPU, held until process exit, so it calls no
  * cudaMalloc.  Limit: ngrain <= 1,048,576, larger calls return BD_ERR_ARG.
- * The first call on a device looks up the scratch address; make it before
- * any stream capture.  All calls on a GPU share the scratch: calls that
- * overlap on the GPU (two streams or threads) race, so serialise them.
- * Device inputs, host output, stream-synchronous. */
+ * The first call on a device looks up the scratch address (a runtime call
+ * that a global-mode stream capture elsewhere in the process would refuse),
+ * so make it before such a capture starts.  The call synchronises its
+ * stream, so it cannot itself be captured.  All calls on a GPU share the
+ * scratch: calls that overlap on the GPU (two streams or threads) race, so
+ * serialise them.  Device inputs, host output, stream-synchronous. */
 int bd_fself_isotropic_noalloc(const float *rr_raw, const float *rr0, int ngrain, float *fself_host,
                                int sample_number, float qmax, void *stream);
 
