@@ -940,54 +940,87 @@ int run_direct(bd_engine *e, int k) {
 // persistent mode) on the live batch and keeps the fastest.  The steps it
 // takes are real steps of the run; results do not depend on the layout
 // (every force sum has a fixed order), only the speed does.
-// List mode: the list-step launch variant (unless the caller fixed it) and
-// the brick shape of the list build, timed together on the live batch over
-// whole steps, rebuilds included as they come.  Neither changes a list or a
-// force sum, so the tuned run's results are those of an untuned run.
+// List mode, in two stages, on the live batch with rebuilds as they come:
+// 1. the list-build brick shape and the per-step launch variant (0-2), each
+//    pair over 2 + 12 steps launched one by one;
+// 2. the winner of stage 1 against the per-replica variants (3-5), each over
+//    one whole graph batch (graph_steps steps, graph instantiated before the
+//    timer starts) after 2 warm-up steps: a per-replica launch pays each
+//    block's cold start and in-block rebuilds once per launch, so a
+//    12-step window does not rank it (it ranks the per-step variants
+//    correctly, whose launches are the same in and out of graphs).
+// Neither choice changes a list or a force sum, so the tuned run's results
+// are those of an untuned run.
 int autotune_list(bd_engine *e, long long &nsteps) {
     static const int shapes[][3] = {{4, 4, 3}, {4, 4, 4}, {3, 3, 3}, {5, 4, 4}, {4, 4, 2}};
     struct Cand { int bx, by, bz, v; };
-    std::vector<Cand> cands;
+    std::vector<Cand> stage1, stage2;
     for (int v = 0; v < kListVariants; v++) {
         if (!(e->tune_lvar || v == e->lvar)) continue;
         if (v >= kListFirstPersistent) {  // builds its lists in the block: no brick shape to choose
-            if (e->rng == BD_RNG_PHILOX) cands.push_back({e->bx, e->by, e->bz, v});
+            if (e->rng == BD_RNG_PHILOX) stage2.push_back({e->bx, e->by, e->bz, v});
             continue;
         }
-        for (auto &sh : shapes) cands.push_back({sh[0], sh[1], sh[2], v});
+        for (auto &sh : shapes) stage1.push_back({sh[0], sh[1], sh[2], v});
     }
     const int warm = 2, timed = 12;
-    if (nsteps < (long long)cands.size() * (warm + timed) + 1) return BD_OK;  // too short to tune now
+    const int n2 = (int)stage2.size() + (stage1.empty() || stage2.empty() ? 0 : 1);
+    const long long need = (long long)stage1.size() * (warm + timed) + (long long)n2 * (warm + e->graph_steps) + 1;
+    if (nsteps < need) return BD_OK;  // too short to tune now
     cudaEvent_t t0, t1;
     BD_CUDA_TRY(cudaEventCreate(&t0));
     BD_CUDA_TRY(cudaEventCreate(&t1));
-    Cand best = {e->bx, e->by, e->bz, e->lvar};
-    float best_ms = 1e30f;
     int rc = BD_OK;
-    for (const Cand &c : cands) {
+    auto apply = [&](const Cand &c) -> int {
         e->bx = c.bx; e->by = c.by; e->bz = c.bz; e->lvar = c.v;
-        if (rebuild_bricks(e) != BD_OK) continue;  // staging of this shape does not fit
-        if ((rc = configure_kernels(e)) != BD_OK) break;
-        if ((rc = upload_layout(e)) != BD_OK) break;
+        if (rebuild_bricks(e) != BD_OK) return -1;  // staging of this shape does not fit
+        int r = configure_kernels(e);
+        return r ? r : upload_layout(e);
+    };
+    auto elapsed = [&](float &ms) -> int {
+        BD_CUDA_TRY(cudaEventRecord(t1, e->stream));
+        if (int r = engine_status(e)) return r;
+        BD_CUDA_TRY(cudaEventElapsedTime(&ms, t0, t1));
+        return BD_OK;
+    };
+    Cand best = {e->bx, e->by, e->bz, e->lvar};
+    float best_ms = 1e30f;  // per step
+    for (const Cand &c : stage1) {
+        const int a = apply(c);
+        if (a < 0) continue;
+        if ((rc = a) != BD_OK) break;
         if ((rc = direct_steps(e, warm)) != BD_OK) break;
         BD_CUDA_TRY(cudaEventRecord(t0, e->stream));
         if ((rc = direct_steps(e, timed)) != BD_OK) break;
-        BD_CUDA_TRY(cudaEventRecord(t1, e->stream));
-        if ((rc = engine_status(e)) != BD_OK) break;
         float ms = 0.f;
-        BD_CUDA_TRY(cudaEventElapsedTime(&ms, t0, t1));
+        if ((rc = elapsed(ms)) != BD_OK) break;
         nsteps -= warm + timed;
-        if (ms < best_ms) { best_ms = ms; best = c; }
+        if (ms / timed < best_ms) { best_ms = ms / timed; best = c; }
+    }
+    if (rc == BD_OK && !stage2.empty()) {
+        if (!stage1.empty()) stage2.insert(stage2.begin(), best);
+        best_ms = 1e30f;
+        for (const Cand &c : stage2) {
+            const int a = apply(c);
+            if (a < 0) continue;
+            if ((rc = a) != BD_OK) break;
+            if ((rc = direct_steps(e, warm)) != BD_OK) break;
+            if ((rc = build_graph(e)) != BD_OK) break;
+            BD_CUDA_TRY(cudaEventRecord(t0, e->stream));
+            BD_CUDA_TRY(cudaGraphLaunch(e->gexec[e->cur], e->stream));
+            e->ni += e->graph_steps;  // cur unchanged: graph_steps is a multiple of 6 in list mode
+            float ms = 0.f;
+            if ((rc = elapsed(ms)) != BD_OK) break;
+            nsteps -= warm + e->graph_steps;
+            if (ms / e->graph_steps < best_ms) { best_ms = ms / e->graph_steps; best = c; }
+        }
     }
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     if (rc) return rc;
-    e->bx = best.bx; e->by = best.by; e->bz = best.bz; e->lvar = best.v;
-    if ((rc = rebuild_bricks(e)) != BD_OK) return rc;
-    if ((rc = configure_kernels(e)) != BD_OK) return rc;
-    if ((rc = upload_layout(e)) != BD_OK) return rc;
+    if ((rc = apply(best)) != BD_OK) return rc < 0 ? BD_ERR_CUDA : rc;
     e->tuned = true;
-    e->tuned_ms = best_ms / timed;
+    e->tuned_ms = best_ms;
     return BD_OK;
 }
 

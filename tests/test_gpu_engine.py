@@ -220,7 +220,7 @@ def test_list_autotuner_and_launch_variants_change_speed_not_results():
     ref = B.Engine(list(systems))
     assert ref.info().neighbor_skin > 0 and ref.info().list_variant == 0
     ref.set_positions(pos)
-    ref.run(400)  # four 96-step graphs and 16 single steps
+    ref.run(700)  # seven 96-step graphs and 28 single steps
     want = ref.get_positions()
     ref_info = ref.info()
     assert ref_info.list_builds > 4 and ref_info.list_rebuild_steps > 1
@@ -229,7 +229,7 @@ def test_list_autotuner_and_launch_variants_change_speed_not_results():
         ev = B.Engine(list(systems), list_variant=v)
         assert ev.info().list_variant == v
         ev.set_positions(pos)
-        ev.run(400)
+        ev.run(700)
         got = ev.get_positions()
         np.testing.assert_array_equal(got[0], want[0], err_msg="variant %d" % v)
         np.testing.assert_array_equal(got[1], want[1], err_msg="variant %d" % v)
@@ -241,7 +241,9 @@ def test_list_autotuner_and_launch_variants_change_speed_not_results():
         ev.close()
     ea = B.Engine(list(systems), autotune=1)
     ea.set_positions(pos)
-    ea.run(400)  # 18 candidates x 14 steps are timed inside the first call
+    # inside the first call: 15 (brick, per-step variant) pairs over 2 + 12
+    # steps, then the best against variants 3-5 over 2 + 96 steps each
+    ea.run(700)
     info = ea.info()
     assert info.tuned_ms > 0 and 0 <= info.list_variant < 6
     got = ea.get_positions()
