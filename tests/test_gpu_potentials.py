@@ -1,7 +1,8 @@
 """The engine with the other pair potentials of potentials.cu (standard WCA,
 WCA 49-50, 49-50 + Asakura-Oosawa depletion, HSAY): energies and virial
 against the oracle's all-pairs forces, one injected-noise step against the
-oracle update (sweep path), and the list path against the sweep path."""
+oracle update (sweep path), the list path against the sweep path, and the
+per-replica list launch against the per-step one."""
 import numpy as np
 import pytest
 
@@ -90,3 +91,39 @@ def test_list_path_tracks_sweep_path(pot, pp):
     d = np.abs(out[0] - out[1])
     d = np.minimum(d, s.side - d)
     assert d.max() < 1e-4, d.max()
+
+
+def test_per_replica_launch_matches_per_step_launch_across_potentials():
+    """The per-replica launch variants (3 and 5: one block per replica that
+    runs a whole graph batch and rebuilds its replica's lists itself) on a
+    batch mixing potentials (the kernels' EXTRA instantiation) and a
+    capped-force replica: the same bits, the same census and the same rebuild
+    counts as the per-step kernels (variant 0), over 300 steps with
+    rebuilds."""
+    specs = [("wca_modified", (0, 0, 0, 0), 0.0), ("ao", (1.0, 0.9, 2.0, 0.2), 0.0), ("hsay", (2.0, 1.6, 0, 0), 0.0),
+             ("wca", (0, 0, 0, 0), 100.0)]
+    systems, poss = [], []
+    for k, (pot, pp, cap) in enumerate(specs):
+        nb = ns = 1500
+        side = float(np.float32(CF.side_from_phi(nb, ns, 0.3)))
+        poss.append(relaxed(nb, ns, side, 20 + k))
+        systems.append(B.System(n_big=nb, n_sml=ns, side=side, sigma_big=SB, sigma_sml=SS, dt=4e-5, seed=20 + k,
+                                T0=1.0, protocol="const", potential=pot, pot_param=pp, force_cap=cap))
+    pos = np.concatenate(poss)
+    out = {}
+    for v in (0, 3, 5):
+        e = B.Engine(systems, list_variant=v)
+        e.set_positions(pos)
+        e.run(300)  # three 96-step graphs and 12 single steps
+        info = e.info()
+        out[v] = (e.get_positions(), e.census(), (info.list_builds, info.list_rebuild_steps))
+        e.close()
+    (hi0, raw0), (cnt0, hsh0), builds0 = out[0]
+    assert builds0[0] > len(systems) and builds0[1] > 1, builds0  # lists were rebuilt during the run
+    for v in (3, 5):
+        (hi, raw), (cnt, hsh), builds = out[v]
+        np.testing.assert_array_equal(hi, hi0, err_msg="variant %d" % v)
+        np.testing.assert_array_equal(raw, raw0, err_msg="variant %d" % v)
+        np.testing.assert_array_equal(cnt, cnt0)
+        np.testing.assert_array_equal(hsh, hsh0)
+        assert builds == builds0, (v, builds, builds0)
