@@ -18,6 +18,7 @@
 #include <new>
 #include <vector>
 
+#include "mlp_chain.cuh"
 #include "runtime.cuh"
 #include "umma.cuh"
 
@@ -75,6 +76,8 @@ int set_gemm_attrs() {
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, umma::kSmemBytes));
     BD_CUDA_TRY(cudaFuncSetAttribute(umma::k_umma_gemm<umma::kEpiBwdGelu>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, umma::kSmemBytes));
+    BD_CUDA_TRY(cudaFuncSetAttribute(umma::k_mlp_chain, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     umma::kChainSmem));
     return BD_OK;
 }
 
@@ -129,70 +132,99 @@ __global__ void k_gather(const float *x, const float *y, int n_data, int n_in, i
             T[(size_t)k * B + r] = (valid && k < n_out) ? y[(size_t)src * n_out + k] : 0.f;
 }
 
-// bias gradient: db[n] = sum over the batch of dZ^T[n][:] (fixed order)
-__global__ void k_bias_grad(const __nv_bfloat16 *dzt, int B, int N, float *db) {
-    const int n = blockIdx.x;
-    float s = 0.f;
-    for (int m = threadIdx.x; m < B; m += blockDim.x) s += __bfloat162float(dzt[(size_t)n * B + m]);
-    __shared__ float red[256];
-    red[threadIdx.x] = s;
-    __syncthreads();
-    for (int off = blockDim.x / 2; off > 0; off >>= 1) {
-        if ((int)threadIdx.x < off) red[threadIdx.x] += red[threadIdx.x + off];
-        __syncthreads();
+// Bias gradients of every layer in one launch: block `row` of the layer
+// table sums dZ_l^T[n][:] over the batch (16-byte loads, a fixed order: the
+// thread's strided slice, then the warp, then the block's warps).
+struct BiasGradArgs {
+    const __nv_bfloat16 *dzt[umma::kChainMaxLayers];  // [N_l][B]
+    float *db[umma::kChainMaxLayers];                 // [N_l]
+    int first[umma::kChainMaxLayers + 1];             // first block of each layer
+    int L, B;                                         // B a multiple of 8
+};
+__global__ void k_bias_grads(const __grid_constant__ BiasGradArgs a) {
+    const int row = blockIdx.x;
+    int l = 0;
+    while (l + 1 < a.L && row >= a.first[l + 1]) l++;
+    const int n = row - a.first[l];
+    const uint4 *src = reinterpret_cast<const uint4 *>(a.dzt[l] + (size_t)n * a.B);
+    float sum = 0.f;
+    for (int i = threadIdx.x; i < a.B / 8; i += blockDim.x) {
+        const uint4 v = src[i];
+        const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&v);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const float2 f = __bfloat1622float2(h[j]);
+            sum += f.x;
+            sum += f.y;
+        }
     }
-    if (threadIdx.x == 0) db[n] = red[0];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, off);
+    __shared__ float red[32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+        a.db[l][n] = t;
+    }
 }
 
 struct AdamArgs {
     float lr, b1, b2, eps;
     const long long *step;  // number of updates so far (incremented by the caller's counter kernel)
+    const float *corr;      // [2]: 1 - b1^t and 1 - b2^t of this update (k_adam_prep)
 };
+// the bias-correction denominators of update t = step + 1, once per step
+__global__ void k_adam_prep(AdamArgs a, float *corr) {
+    const float t = (float)(*a.step + 1);
+    corr[0] = 1.f - powf(a.b1, t);
+    corr[1] = 1.f - powf(a.b2, t);
+}
 
-// Adam on one weight matrix W [N][K] (gradient = sum of the split partials,
-// stored transposed [splits][K][N] by the weight-gradient GEMM) and its
-// bias; writes the BF16 copies W [N][K] and W^T [K][N].
+// Adam on one weight matrix (gradient = sum of the split partials, stored
+// [splits][K][N] by the weight-gradient GEMM) in [k][n] order: the FP32
+// master weights and the moments are kept in that order too, so every FP32
+// access is coalesced; writes the BF16 copies W [N][K] and W^T [K][N].
 __global__ void k_adam(float *w, float *m1, float *m2, const float *part, int splits, int N, int K, int n_live,
                        int k_live, __nv_bfloat16 *wb, __nv_bfloat16 *wbt, AdamArgs a) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // [k][n] order
     if (i >= (size_t)N * K) return;
     const int k = (int)(i / N), n = (int)(i % N);
-    const size_t wi = (size_t)n * K + k;
     float gsum = 0.f;
     for (int s = 0; s < splits; s++) gsum += part[(size_t)s * N * K + i];
-    const float t = (float)(*a.step + 1);
-    float wv = w[wi];
+    float wv = w[i];
     if (n < n_live && k < k_live) {
-        const float mm = a.b1 * m1[wi] + (1.f - a.b1) * gsum;
-        const float vv = a.b2 * m2[wi] + (1.f - a.b2) * gsum * gsum;
-        m1[wi] = mm;
-        m2[wi] = vv;
-        const float mh = mm / (1.f - powf(a.b1, t)), vh = vv / (1.f - powf(a.b2, t));
+        const float mm = a.b1 * m1[i] + (1.f - a.b1) * gsum;
+        const float vv = a.b2 * m2[i] + (1.f - a.b2) * gsum * gsum;
+        m1[i] = mm;
+        m2[i] = vv;
+        const float mh = mm / a.corr[0], vh = vv / a.corr[1];
         wv -= a.lr * mh / (sqrtf(vh) + a.eps);
-        w[wi] = wv;
+        w[i] = wv;
     }
     const __nv_bfloat16 b = __float2bfloat16_rn(wv);
-    wb[wi] = b;
+    wb[(size_t)n * K + k] = b;
     wbt[i] = b;
 }
 __global__ void k_adam_bias(float *b, float *m1, float *m2, const float *g, int N, int n_live, AdamArgs a) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= N || n >= n_live) return;
-    const float t = (float)(*a.step + 1);
     const float mm = a.b1 * m1[n] + (1.f - a.b1) * g[n];
     const float vv = a.b2 * m2[n] + (1.f - a.b2) * g[n] * g[n];
     m1[n] = mm;
     m2[n] = vv;
-    b[n] -= a.lr * (mm / (1.f - powf(a.b1, t))) / (sqrtf(vv / (1.f - powf(a.b2, t))) + a.eps);
+    b[n] -= a.lr * (mm / a.corr[0]) / (sqrtf(vv / a.corr[1]) + a.eps);
 }
 __global__ void k_count(long long *step) { *step += 1; }
+// BF16 copies W [N][K] and W^T [K][N] of the FP32 master weights (kept [K][N])
 __global__ void k_to_bf16(const float *w, int N, int K, __nv_bfloat16 *wb, __nv_bfloat16 *wbt) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // [k][n] order
     if (i >= (size_t)N * K) return;
-    const int n = (int)(i / K), k = (int)(i % K);
+    const int k = (int)(i / N), n = (int)(i % N);
     const __nv_bfloat16 b = __float2bfloat16_rn(w[i]);
-    wb[i] = b;
-    wbt[(size_t)k * N + n] = b;
+    wb[(size_t)n * K + k] = b;
+    wbt[i] = b;
 }
 
 }  // namespace
@@ -207,7 +239,7 @@ struct bd_surrogate {
     std::vector<int> Kp, Np;          // padded input / output sizes per layer
     std::vector<int> Kl, Nl;          // live sizes
     cudaStream_t stream = nullptr;
-    // parameters (FP32 master + Adam moments), BF16 copies
+    // parameters (FP32 master weights [K][N] and Adam moments in that order, biases), BF16 copies
     std::vector<float *> w, b, wm, wv, bm, bv;
     std::vector<__nv_bfloat16 *> wb, wbt;
     // activations (BF16 row-major and transposed), pre-activations FP32
@@ -219,11 +251,16 @@ struct bd_surrogate {
     std::vector<float *> db;          // bias gradients
     float *loss_part = nullptr;
     long long *step = nullptr;
+    float *corr = nullptr;            // Adam bias-correction denominators of the current update
     unsigned *err = nullptr;
     float *data_x = nullptr, *data_y = nullptr;
     int n_data = 0;
     unsigned long long seed = 1;
     std::vector<CUtensorMap> tm_h, tm_ht, tm_dz, tm_dzt, tm_wb, tm_wbt;
+    // the fused forward / input-gradient kernel (k_mlp_chain): W_l and W_l^T
+    // as whole-height boxes
+    std::vector<CUtensorMap> tm_wfull, tm_wtfull;
+    bool chain = false;
     cudaGraphExec_t graph = nullptr;
     float lr = 1e-3f;
     int loss_cells = 0;
@@ -251,7 +288,8 @@ void free_surrogate(bd_surrogate *s) {
     for (auto *p : s->dz) F(p);
     for (auto *p : s->dzt) F(p);
     for (auto *p : s->db) F(p);
-    F(s->y); F(s->t); F(s->tw); F(s->part); F(s->loss_part); F(s->step); F(s->err); F(s->data_x); F(s->data_y);
+    F(s->y); F(s->t); F(s->tw); F(s->part); F(s->loss_part); F(s->step); F(s->corr); F(s->err); F(s->data_x);
+    F(s->data_y);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
@@ -271,9 +309,54 @@ GemmArgs base_args(bd_surrogate *s) {
     return g;
 }
 
+// The forward pass of every 128-row block of the batch, and in training its
+// loss gradient and input-gradient chain (dZ_l for every layer), in one
+// launch of k_mlp_chain (a cluster of four CTAs per block).
+int chain_launch(bd_surrogate *s, bool train) {
+    umma::ChainMaps maps;
+    std::memset(&maps, 0, sizeof(maps));
+    maps.x = s->tm_h[0];
+    umma::ChainArgs g;
+    std::memset(&g, 0, sizeof(g));
+    g.L = s->L;
+    g.M = s->batch;
+    g.backward = train ? 1 : 0;
+    for (int l = 0; l < s->L; l++) {
+        maps.w[l] = s->tm_wfull[l];
+        maps.wt[l] = s->tm_wtfull[l];
+        const bool hidden = l < s->L - 1;
+        g.lay[l] = {s->Kp[l], s->Np[l], s->b[l], hidden ? s->z[l] : s->y, hidden ? s->ht[l + 1] : nullptr, s->dzt[l]};
+    }
+    if (train) {
+        g.target = s->t;
+        g.tweight = s->tw;
+        g.n_valid = s->n_out;
+        g.grad_scale = 2.0f / ((float)s->batch * (float)s->n_out);
+        g.loss_part = s->loss_part;
+    }
+    g.err = s->err;
+    cudaLaunchConfig_t cfg;
+    std::memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3((s->batch / kBM) * umma::kChainCluster);
+    cfg.blockDim = dim3(umma::kChainThreads);
+    cfg.dynamicSmemBytes = umma::kChainSmem;
+    cfg.stream = s->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = umma::kChainCluster;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    BD_CUDA_TRY(cudaLaunchKernelEx(&cfg, umma::k_mlp_chain, maps, g));
+    return BD_OK;
+}
+
 // forward of the whole network on the batch in h[0]; with a target the last
-// epilogue writes the loss gradient dz[L-1]
+// epilogue writes the loss gradient dz[L-1] (and the fused kernel also runs
+// the input-gradient chain)
 int forward(bd_surrogate *s, bool with_target) {
+    if (s->chain) return chain_launch(s, with_target);
     const int B = s->batch;
     for (int l = 0; l < s->L; l++) {
         GemmArgs g = base_args(s);
@@ -327,9 +410,7 @@ int backward(bd_surrogate *s) {
         g.out_f32 = s->part + part_offset(s, l);
         int rc = launch_gemm<umma::kEpiF32>(s->tm_dzt[l], s->tm_ht[l], g, s->stream);
         if (rc) return rc;
-        k_bias_grad<<<s->Np[l], 256, 0, s->stream>>>(s->dzt[l], B, s->Np[l], s->db[l]);
-        BD_LAUNCH_CHECK();
-        if (l == 0) break;
+        if (l == 0 || s->chain) continue;  // the fused forward kernel wrote every dZ_l already
         // dH_{l-1} = dZ_l W_l, times gelu'(Z_{l-1})
         GemmArgs d = base_args(s);
         d.M = B;
@@ -342,11 +423,23 @@ int backward(bd_surrogate *s) {
         rc = launch_gemm<umma::kEpiBwdGelu>(s->tm_dz[l], s->tm_wbt[l], d, s->stream);
         if (rc) return rc;
     }
+    BiasGradArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.L = s->L;
+    a.B = B;
+    for (int l = 0; l < s->L; l++) {
+        a.dzt[l] = s->dzt[l];
+        a.db[l] = s->db[l];
+        a.first[l + 1] = a.first[l] + s->Np[l];
+    }
+    k_bias_grads<<<a.first[s->L], 256, 0, s->stream>>>(a);
+    BD_LAUNCH_CHECK();
     return BD_OK;
 }
 
 int adam(bd_surrogate *s) {
-    AdamArgs a{s->lr, 0.9f, 0.999f, 1e-8f, s->step};
+    AdamArgs a{s->lr, 0.9f, 0.999f, 1e-8f, s->step, s->corr};
+    k_adam_prep<<<1, 1, 0, s->stream>>>(a, s->corr);
     const int splits = s->batch / s->ksplit;
     for (int l = 0; l < s->L; l++) {
         const size_t n = (size_t)s->Np[l] * s->Kp[l];
@@ -396,6 +489,8 @@ int bd_surrogate_create(int n_in, int n_out, int width, int depth, int batch, un
         s->Nl.push_back(l == s->L - 1 ? n_out : width);
         s->Np.push_back(l == s->L - 1 ? 128 : width);
     }
+    // the fused forward / input-gradient kernel covers every shape accepted here
+    s->chain = s->L <= umma::kChainMaxLayers && batch % kBM == 0;
     if (set_gemm_attrs() != BD_OK || cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete s;
         return BD_ERR_CUDA;
@@ -430,9 +525,12 @@ int bd_surrogate_create(int n_in, int n_out, int width, int depth, int batch, un
     A((void **)&s->t, (size_t)batch * 128 * 4);
     A((void **)&s->tw, 128 * 4);
     A((void **)&s->part, part_total * 4);
-    s->loss_cells = (batch / kBM) * div_up(s->Np[s->L - 1], kBN);  // CTAs of the output GEMM
+    // loss partials: one per CTA of the output GEMM, or per block of the fused kernel
+    s->loss_cells = (batch / kBM) * std::max(div_up(s->Np[s->L - 1], kBN), umma::kChainCluster);
     A((void **)&s->loss_part, (size_t)s->loss_cells * 4);
+    if (s->chain) s->loss_cells = (batch / kBM) * umma::kChainCluster;
     A((void **)&s->step, sizeof(long long));
+    A((void **)&s->corr, 2 * sizeof(float));
     A((void **)&s->err, sizeof(unsigned));
     if (!ok) {
         free_surrogate(s);
@@ -448,7 +546,7 @@ int bd_surrogate_create(int n_in, int n_out, int width, int depth, int batch, un
         std::vector<float> hw((size_t)s->Np[l] * s->Kp[l], 0.f);
         const double scale = std::sqrt(6.0 / (double)s->Kl[l]);
         for (int n = 0; n < s->Nl[l]; n++)
-            for (int k = 0; k < s->Kl[l]; k++) hw[(size_t)n * s->Kp[l] + k] = (float)(scale * rnd() * 0.5);
+            for (int k = 0; k < s->Kl[l]; k++) hw[(size_t)k * s->Np[l] + n] = (float)(scale * rnd() * 0.5);
         cudaMemcpyAsync(s->w[l], hw.data(), hw.size() * 4, cudaMemcpyHostToDevice, s->stream);
         k_to_bf16<<<div_up((long)hw.size(), 256), 256, 0, s->stream>>>(s->w[l], s->Np[l], s->Kp[l], s->wb[l],
                                                                        s->wbt[l]);
@@ -472,6 +570,14 @@ int bd_surrogate_create(int n_in, int n_out, int width, int depth, int batch, un
         rc |= make_tmap(&s->tm_dzt[l], s->dzt[l], s->Np[l], batch, kBM);
         rc |= make_tmap(&s->tm_wb[l], s->wb[l], s->Np[l], s->Kp[l], kBN);
         rc |= make_tmap(&s->tm_wbt[l], s->wbt[l], s->Kp[l], s->Np[l], kBN);
+    }
+    if (s->chain) {  // the fused kernel's weight boxes: a quarter of the rows per CTA of a cluster
+        s->tm_wfull.resize(s->L);
+        s->tm_wtfull.resize(s->L);
+        for (int l = 0; l < s->L && !rc; l++) {
+            rc |= make_tmap(&s->tm_wfull[l], s->wb[l], s->Np[l], s->Kp[l], s->Np[l] / umma::kChainCluster);
+            rc |= make_tmap(&s->tm_wtfull[l], s->wbt[l], s->Kp[l], s->Np[l], s->Kp[l] / umma::kChainCluster);
+        }
     }
     if (rc || cudaStreamSynchronize(s->stream) != cudaSuccess) {
         free_surrogate(s);
@@ -512,7 +618,7 @@ int bd_surrogate_get_params(bd_surrogate *s, float *out) {
         BD_CUDA_TRY(cudaMemcpyAsync(hb.data(), s->b[l], hb.size() * 4, cudaMemcpyDeviceToHost, s->stream));
         BD_CUDA_TRY(cudaStreamSynchronize(s->stream));
         for (int n = 0; n < s->Nl[l]; n++)
-            for (int k = 0; k < s->Kl[l]; k++) out[off++] = hw[(size_t)n * s->Kp[l] + k];
+            for (int k = 0; k < s->Kl[l]; k++) out[off++] = hw[(size_t)k * s->Np[l] + n];  // master kept [K][N]
         for (int n = 0; n < s->Nl[l]; n++) out[off++] = hb[n];
     }
     return BD_OK;
@@ -524,7 +630,7 @@ int bd_surrogate_set_params(bd_surrogate *s, const float *in) {
     for (int l = 0; l < s->L; l++) {
         std::vector<float> hw((size_t)s->Np[l] * s->Kp[l], 0.f), hb(s->Np[l], 0.f);
         for (int n = 0; n < s->Nl[l]; n++)
-            for (int k = 0; k < s->Kl[l]; k++) hw[(size_t)n * s->Kp[l] + k] = in[off++];
+            for (int k = 0; k < s->Kl[l]; k++) hw[(size_t)k * s->Np[l] + n] = in[off++];  // master kept [K][N]
         for (int n = 0; n < s->Nl[l]; n++) hb[n] = in[off++];
         BD_CUDA_TRY(cudaMemcpyAsync(s->w[l], hw.data(), hw.size() * 4, cudaMemcpyHostToDevice, s->stream));
         BD_CUDA_TRY(cudaMemcpyAsync(s->b[l], hb.data(), hb.size() * 4, cudaMemcpyHostToDevice, s->stream));

@@ -347,8 +347,9 @@ def surrogate_flops(sizes, batch):
 def surrogate_leg(steps=200, warmup=20, batch=4096):
     """Training steps of the surrogate (5 -> 256 x 4 -> 34, GELU, batch 4096,
     Adam) on a synthetic 1e5-sample set, each step one CUDA graph of
-    gather, 5 forward GEMMs, 5 weight-gradient and 4 input-gradient GEMMs,
-    bias gradients and Adam."""
+    gather, the fused forward and input-gradient kernel (the 5 forward and 4
+    input-gradient GEMMs in one launch), 5 weight-gradient GEMMs, bias
+    gradients and Adam."""
     from bd_aging_b200 import lib as B
     import torch
     rng = np.random.default_rng(0)
@@ -370,7 +371,7 @@ def surrogate_leg(steps=200, warmup=20, batch=4096):
     return {"ms_per_train_step": ms, "useful_tflops": useful / (ms / 1e3) / 1e12,
             "executed_tflops": executed / (ms / 1e3) / 1e12, "gflop_per_step_useful": useful / 1e9,
             "gflop_per_step_executed": executed / 1e9, "batch": batch, "final_loss": loss,
-            "gemm_launches_per_step": 14}
+            "gemm_launches_per_step": 6, "gemms_per_step": 14}
 
 
 def surrogate_quality_leg():

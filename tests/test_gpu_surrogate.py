@@ -34,7 +34,7 @@ def _net(width, depth, batch, seed=3, n_in=5, n_out=34):
     return s, layers, x, t
 
 
-@pytest.mark.parametrize("width,depth,batch", [(64, 2, 256), (256, 4, 4096)])
+@pytest.mark.parametrize("width,depth,batch", [(64, 2, 256), (192, 3, 512), (256, 4, 4096)])
 def test_gradients_match_oracle(width, depth, batch):
     s, layers, x, t = _net(width, depth, batch)
     g, loss = s.gradients(x.astype(np.float32), t.astype(np.float32))
