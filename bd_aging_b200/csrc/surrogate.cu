@@ -1,15 +1,19 @@
 // surrogate.cu -- the learned surrogate: an MLP n_in -> width (GELU) x depth
 // -> n_out trained and evaluated by hand-written tcgen05 BF16 GEMMs with FP32
-// accumulation (umma.cuh), Adam in FP32 on FP32 master weights.
+// accumulation, Adam in FP32 on FP32 master weights.
 //
 // Per layer l (K_l inputs, N_l outputs, batch B) every GEMM has both
 // operands K-major; the transposed copies it needs are written by the
 // epilogue or the optimizer that produces them:
 //   forward   Z_l  = H_{l-1} W_l^T + b_l        A = H_{l-1} [B][K_l], B = W_l  [N_l][K_l]
-//   weights   dW_l = dZ_l^T H_{l-1}             A = dZ_l^T  [N_l][B], B = H_{l-1}^T [K_l][B]
 //   input     dH_{l-1} = dZ_l W_l               A = dZ_l    [B][N_l], B = W_l^T [K_l][N_l]
-// dW is split over the batch (256 rows per CTA) into FP32 partials that the
-// Adam kernel adds in a fixed order, so a training step is deterministic.
+//   weights   dW_l = dZ_l^T H_{l-1}             A = dZ_l^T  [N_l][B], B = H_{l-1}^T [K_l][B]
+// The forward and input-gradient GEMMs of a training step run in one launch
+// of the fused kernel (mlp_chain.cuh), which keeps each 128-row block's
+// activations and gradients in shared memory and writes H_l^T and dZ_l^T for
+// the weight-gradient GEMMs (umma.cuh).  dW is split over the batch (256
+// rows per CTA) into FP32 partials that the Adam kernel adds in a fixed
+// order, so a training step is deterministic.
 #include <cuda.h>
 #include <cuda_bf16.h>
 
@@ -65,27 +69,20 @@ int make_tmap(CUtensorMap *map, const void *ptr, int rows, int cols, int box_row
     return r == CUDA_SUCCESS ? BD_OK : BD_ERR_ARG;
 }
 
-// dynamic shared memory above 48 KB for every GEMM variant; called outside
-// stream capture (create, direct GEMM)
+// dynamic shared memory above 48 KB for the GEMM and the fused kernel;
+// called outside stream capture (create, direct GEMM)
 int set_gemm_attrs() {
-    BD_CUDA_TRY(cudaFuncSetAttribute(umma::k_umma_gemm<umma::kEpiF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    BD_CUDA_TRY(cudaFuncSetAttribute(umma::k_umma_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      umma::kSmemBytes));
-    BD_CUDA_TRY(cudaFuncSetAttribute(umma::k_umma_gemm<umma::kEpiFwdGelu>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, umma::kSmemBytes));
-    BD_CUDA_TRY(cudaFuncSetAttribute(umma::k_umma_gemm<umma::kEpiFwdOut>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, umma::kSmemBytes));
-    BD_CUDA_TRY(cudaFuncSetAttribute(umma::k_umma_gemm<umma::kEpiBwdGelu>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, umma::kSmemBytes));
     BD_CUDA_TRY(cudaFuncSetAttribute(umma::k_mlp_chain, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      umma::kChainSmem));
     return BD_OK;
 }
 
-template <int EPI>
 int launch_gemm(const CUtensorMap &a, const CUtensorMap &b, const GemmArgs &g, cudaStream_t st) {
     if (g.k_split % kBK || g.k_split > umma::kMaxChunks * kBK || g.k_split < kBK) return BD_ERR_ARG;
     dim3 grid(div_up(g.M, kBM), div_up(g.N, kBN), div_up(g.K, g.k_split));
-    umma::k_umma_gemm<EPI><<<grid, umma::kThreads, umma::kSmemBytes, st>>>(a, b, g);
+    umma::k_umma_gemm<<<grid, umma::kThreads, umma::kSmemBytes, st>>>(a, b, g);
     BD_LAUNCH_CHECK();
     return BD_OK;
 }
@@ -243,9 +240,10 @@ struct bd_surrogate {
     std::vector<float *> w, b, wm, wv, bm, bv;
     std::vector<__nv_bfloat16 *> wb, wbt;
     // activations (BF16 row-major and transposed), pre-activations FP32
-    std::vector<__nv_bfloat16 *> h, ht;   // h[0] = input X0; h[l+1] = output of layer l (hidden)
+    __nv_bfloat16 *x0 = nullptr;          // input X0 [B][K_0]
+    std::vector<__nv_bfloat16 *> ht;      // ht[0] = X0^T; ht[l+1] = H_l^T, output of hidden layer l [N_l][B]
     std::vector<float *> z;               // z[l] pre-activation of layer l, transposed [N_l][B]
-    std::vector<__nv_bfloat16 *> dz, dzt; // dz[l] gradient w.r.t. z[l]
+    std::vector<__nv_bfloat16 *> dzt;     // dZ_l^T, gradient w.r.t. z[l] [N_l][B]
     float *y = nullptr, *t = nullptr, *tw = nullptr;  // output [128][B], target [128][B] (transposed), weights
     float *part = nullptr;            // weight-gradient split partials [splits][K_l][N_l] per layer
     std::vector<float *> db;          // bias gradients
@@ -256,11 +254,11 @@ struct bd_surrogate {
     float *data_x = nullptr, *data_y = nullptr;
     int n_data = 0;
     unsigned long long seed = 1;
-    std::vector<CUtensorMap> tm_h, tm_ht, tm_dz, tm_dzt, tm_wb, tm_wbt;
-    // the fused forward / input-gradient kernel (k_mlp_chain): W_l and W_l^T
-    // as whole-height boxes
-    std::vector<CUtensorMap> tm_wfull, tm_wtfull;
-    bool chain = false;
+    // TMA maps: X0 (box 128 rows), the weight-gradient GEMMs' operands dZ_l^T and
+    // H_{l-1}^T, and W_l, W_l^T in boxes of a quarter of their rows (one CTA of a
+    // fused kernel's cluster each)
+    CUtensorMap tm_x;
+    std::vector<CUtensorMap> tm_ht, tm_dzt, tm_w, tm_wt;
     cudaGraphExec_t graph = nullptr;
     float lr = 1e-3f;
     int loss_cells = 0;
@@ -282,13 +280,11 @@ void free_surrogate(bd_surrogate *s) {
     for (auto *p : s->bv) F(p);
     for (auto *p : s->wb) F(p);
     for (auto *p : s->wbt) F(p);
-    for (auto *p : s->h) F(p);
     for (auto *p : s->ht) F(p);
     for (auto *p : s->z) F(p);
-    for (auto *p : s->dz) F(p);
     for (auto *p : s->dzt) F(p);
     for (auto *p : s->db) F(p);
-    F(s->y); F(s->t); F(s->tw); F(s->part); F(s->loss_part); F(s->step); F(s->corr); F(s->err); F(s->data_x);
+    F(s->x0); F(s->y); F(s->t); F(s->tw); F(s->part); F(s->loss_part); F(s->step); F(s->corr); F(s->err); F(s->data_x);
     F(s->data_y);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -315,15 +311,15 @@ GemmArgs base_args(bd_surrogate *s) {
 int chain_launch(bd_surrogate *s, bool train) {
     umma::ChainMaps maps;
     std::memset(&maps, 0, sizeof(maps));
-    maps.x = s->tm_h[0];
+    maps.x = s->tm_x;
     umma::ChainArgs g;
     std::memset(&g, 0, sizeof(g));
     g.L = s->L;
     g.M = s->batch;
     g.backward = train ? 1 : 0;
     for (int l = 0; l < s->L; l++) {
-        maps.w[l] = s->tm_wfull[l];
-        maps.wt[l] = s->tm_wtfull[l];
+        maps.w[l] = s->tm_w[l];
+        maps.wt[l] = s->tm_wt[l];
         const bool hidden = l < s->L - 1;
         g.lay[l] = {s->Kp[l], s->Np[l], s->b[l], hidden ? s->z[l] : s->y, hidden ? s->ht[l + 1] : nullptr, s->dzt[l]};
     }
@@ -352,43 +348,9 @@ int chain_launch(bd_surrogate *s, bool train) {
     return BD_OK;
 }
 
-// forward of the whole network on the batch in h[0]; with a target the last
-// epilogue writes the loss gradient dz[L-1] (and the fused kernel also runs
-// the input-gradient chain)
-int forward(bd_surrogate *s, bool with_target) {
-    if (s->chain) return chain_launch(s, with_target);
-    const int B = s->batch;
-    for (int l = 0; l < s->L; l++) {
-        GemmArgs g = base_args(s);
-        g.M = B;
-        g.N = s->Np[l];
-        g.K = s->Kp[l];
-        g.k_split = std::min(256, ((g.K + kBK - 1) / kBK) * kBK);
-        g.bias = s->b[l];
-        int rc;
-        if (l < s->L - 1) {
-            g.out_f32 = s->z[l];
-            g.out_bf = s->h[l + 1];
-            g.out_bfT = s->ht[l + 1];
-            rc = launch_gemm<umma::kEpiFwdGelu>(s->tm_h[l], s->tm_wb[l], g, s->stream);
-        } else {
-            g.out_f32 = s->y;
-            if (with_target) {
-                g.target = s->t;
-                g.tweight = s->tw;
-                g.m_valid = B;
-                g.n_valid = s->n_out;
-                g.grad_scale = 2.0f / ((float)B * (float)s->n_out);
-                g.out_bf = s->dz[l];
-                g.out_bfT = s->dzt[l];
-                g.loss_part = s->loss_part;
-            }
-            rc = launch_gemm<umma::kEpiFwdOut>(s->tm_h[l], s->tm_wb[l], g, s->stream);
-        }
-        if (rc) return rc;
-    }
-    return BD_OK;
-}
+// forward of the whole network on the batch in h[0]; with a target also the
+// loss gradient and every dZ_l (the fused kernel's input-gradient chain)
+int forward(bd_surrogate *s, bool with_target) { return chain_launch(s, with_target); }
 
 // gradients of every layer into the split partials and db; dW_l partials go
 // to part + offset(l)
@@ -398,6 +360,8 @@ size_t part_offset(const bd_surrogate *s, int l) {
     return off;
 }
 
+// weight and bias gradients from the dZ_l^T and H_{l-1}^T the forward
+// launch wrote
 int backward(bd_surrogate *s) {
     const int B = s->batch;
     for (int l = s->L - 1; l >= 0; l--) {
@@ -408,19 +372,7 @@ int backward(bd_surrogate *s) {
         g.K = B;
         g.k_split = s->ksplit;
         g.out_f32 = s->part + part_offset(s, l);
-        int rc = launch_gemm<umma::kEpiF32>(s->tm_dzt[l], s->tm_ht[l], g, s->stream);
-        if (rc) return rc;
-        if (l == 0 || s->chain) continue;  // the fused forward kernel wrote every dZ_l already
-        // dH_{l-1} = dZ_l W_l, times gelu'(Z_{l-1})
-        GemmArgs d = base_args(s);
-        d.M = B;
-        d.N = s->Kp[l];
-        d.K = s->Np[l];
-        d.k_split = std::min(256, d.K);
-        d.zin = s->z[l - 1];
-        d.out_bf = s->dz[l - 1];
-        d.out_bfT = s->dzt[l - 1];
-        rc = launch_gemm<umma::kEpiBwdGelu>(s->tm_dz[l], s->tm_wbt[l], d, s->stream);
+        int rc = launch_gemm(s->tm_dzt[l], s->tm_ht[l], g, s->stream);
         if (rc) return rc;
     }
     BiasGradArgs a;
@@ -456,7 +408,7 @@ int adam(bd_surrogate *s) {
 
 int train_step_launches(bd_surrogate *s) {
     k_gather<<<s->batch, 64, 0, s->stream>>>(s->data_x, s->data_y, s->n_data, s->n_in, s->n_out, s->Kp[0],
-                                             s->Np[s->L - 1], s->batch, nullptr, s->step, s->seed, s->h[0], s->ht[0],
+                                             s->Np[s->L - 1], s->batch, nullptr, s->step, s->seed, s->x0, s->ht[0],
                                              s->t);
     BD_LAUNCH_CHECK();
     int rc = forward(s, true);
@@ -490,7 +442,7 @@ int bd_surrogate_create(int n_in, int n_out, int width, int depth, int batch, un
         s->Np.push_back(l == s->L - 1 ? 128 : width);
     }
     // the fused forward / input-gradient kernel covers every shape accepted here
-    s->chain = s->L <= umma::kChainMaxLayers && batch % kBM == 0;
+    static_assert(8 + 1 <= umma::kChainMaxLayers && 256 % kBM == 0, "depth <= 8, batch a multiple of 256");
     if (set_gemm_attrs() != BD_OK || cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete s;
         return BD_ERR_CUDA;
@@ -514,10 +466,9 @@ int bd_surrogate_create(int n_in, int n_out, int width, int depth, int batch, un
         A((void **)&p, s->Np[l] * 4); s->db.push_back(p);
         A((void **)&q, nk * 2); s->wb.push_back(q);
         A((void **)&q, nk * 2); s->wbt.push_back(q);
-        A((void **)&q, (size_t)batch * s->Kp[l] * 2); s->h.push_back(q);
+        if (l == 0) A((void **)&s->x0, (size_t)batch * s->Kp[0] * 2);
         A((void **)&q, (size_t)batch * s->Kp[l] * 2); s->ht.push_back(q);
         A((void **)&p, (size_t)batch * s->Np[l] * 4); s->z.push_back(p);
-        A((void **)&q, (size_t)batch * s->Np[l] * 2); s->dz.push_back(q);
         A((void **)&q, (size_t)batch * s->Np[l] * 2); s->dzt.push_back(q);
         part_total += (size_t)(batch / s->ksplit) * nk;
     }
@@ -525,10 +476,9 @@ int bd_surrogate_create(int n_in, int n_out, int width, int depth, int batch, un
     A((void **)&s->t, (size_t)batch * 128 * 4);
     A((void **)&s->tw, 128 * 4);
     A((void **)&s->part, part_total * 4);
-    // loss partials: one per CTA of the output GEMM, or per block of the fused kernel
-    s->loss_cells = (batch / kBM) * std::max(div_up(s->Np[s->L - 1], kBN), umma::kChainCluster);
+    // loss partials: one per CTA of the fused kernel
+    s->loss_cells = (batch / kBM) * umma::kChainCluster;
     A((void **)&s->loss_part, (size_t)s->loss_cells * 4);
-    if (s->chain) s->loss_cells = (batch / kBM) * umma::kChainCluster;
     A((void **)&s->step, sizeof(long long));
     A((void **)&s->corr, 2 * sizeof(float));
     A((void **)&s->err, sizeof(unsigned));
@@ -555,29 +505,18 @@ int bd_surrogate_create(int n_in, int n_out, int width, int depth, int batch, un
     cudaMemcpyAsync(s->tw, ones.data(), 128 * 4, cudaMemcpyHostToDevice, s->stream);
     // tensor maps
     int rc = BD_OK;
-    s->tm_h.resize(s->L);
     s->tm_ht.resize(s->L);
-    s->tm_dz.resize(s->L);
     s->tm_dzt.resize(s->L);
-    s->tm_wb.resize(s->L);
-    s->tm_wbt.resize(s->L);
+    s->tm_w.resize(s->L);
+    s->tm_wt.resize(s->L);
+    rc |= make_tmap(&s->tm_x, s->x0, batch, s->Kp[0], kBM);
     for (int l = 0; l < s->L && !rc; l++) {
-        // A operands: h (forward), dz^T (weight gradient), dz (input gradient);
-        // B operands: W, h^T, W^T
-        rc |= make_tmap(&s->tm_h[l], s->h[l], batch, s->Kp[l], kBM);
-        rc |= make_tmap(&s->tm_ht[l], s->ht[l], s->Kp[l], batch, kBN);
-        rc |= make_tmap(&s->tm_dz[l], s->dz[l], batch, s->Np[l], kBM);
+        // weight gradient: A = dZ_l^T, B = H_{l-1}^T; fused kernel: W_l and W_l^T,
+        // a quarter of the rows per CTA of a cluster
         rc |= make_tmap(&s->tm_dzt[l], s->dzt[l], s->Np[l], batch, kBM);
-        rc |= make_tmap(&s->tm_wb[l], s->wb[l], s->Np[l], s->Kp[l], kBN);
-        rc |= make_tmap(&s->tm_wbt[l], s->wbt[l], s->Kp[l], s->Np[l], kBN);
-    }
-    if (s->chain) {  // the fused kernel's weight boxes: a quarter of the rows per CTA of a cluster
-        s->tm_wfull.resize(s->L);
-        s->tm_wtfull.resize(s->L);
-        for (int l = 0; l < s->L && !rc; l++) {
-            rc |= make_tmap(&s->tm_wfull[l], s->wb[l], s->Np[l], s->Kp[l], s->Np[l] / umma::kChainCluster);
-            rc |= make_tmap(&s->tm_wtfull[l], s->wbt[l], s->Kp[l], s->Np[l], s->Kp[l] / umma::kChainCluster);
-        }
+        rc |= make_tmap(&s->tm_ht[l], s->ht[l], s->Kp[l], batch, kBN);
+        rc |= make_tmap(&s->tm_w[l], s->wb[l], s->Np[l], s->Kp[l], s->Np[l] / umma::kChainCluster);
+        rc |= make_tmap(&s->tm_wt[l], s->wbt[l], s->Kp[l], s->Np[l], s->Kp[l] / umma::kChainCluster);
     }
     if (rc || cudaStreamSynchronize(s->stream) != cudaSuccess) {
         free_surrogate(s);
@@ -714,7 +653,7 @@ int bd_surrogate_gradients(bd_surrogate *s, const float *x, const float *y, floa
     BD_CUDA_TRY(cudaMalloc(&drows, B * 4));
     cudaMemcpyAsync(drows, rows.data(), B * 4, cudaMemcpyHostToDevice, s->stream);
     k_gather<<<B, 64, 0, s->stream>>>(dx, dy, B, s->n_in, s->n_out, s->Kp[0], s->Np[s->L - 1], B, drows, s->step,
-                                      s->seed, s->h[0], s->ht[0], s->t);
+                                      s->seed, s->x0, s->ht[0], s->t);
     int rc = forward(s, true);
     if (!rc) rc = backward(s);
     const int splits = B / s->ksplit;
@@ -767,7 +706,7 @@ int bd_surrogate_predict(bd_surrogate *s, const float *x, int n, float *y) {
         for (int i = 0; i < B; i++) rows[i] = i < cnt ? r0 + i : -1;
         cudaMemcpyAsync(drows, rows.data(), B * 4, cudaMemcpyHostToDevice, s->stream);
         k_gather<<<B, 64, 0, s->stream>>>(dx, nullptr, n, s->n_in, s->n_out, s->Kp[0], s->Np[s->L - 1], B, drows,
-                                          s->step, s->seed, s->h[0], s->ht[0], nullptr);
+                                          s->step, s->seed, s->x0, s->ht[0], nullptr);
         rc = forward(s, false);
         if (rc) break;
         cudaMemcpyAsync(hy.data(), s->y, hy.size() * 4, cudaMemcpyDeviceToHost, s->stream);
@@ -814,7 +753,7 @@ int bd_umma_gemm_bf16(const unsigned short *a, const unsigned short *b, int M, i
         g.k_split = ks;
         g.out_f32 = part;
         g.err = err;
-        rc = launch_gemm<umma::kEpiF32>(ta, tb, g, st);
+        rc = launch_gemm(ta, tb, g, st);
     }
     if (!rc) {
         k_sum_splits<<<div_up((long)M * N, 256), 256, 0, st>>>(part, splits, (size_t)M * N, dc);

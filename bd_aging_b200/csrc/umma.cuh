@@ -1,6 +1,8 @@
 // umma.cuh -- BF16 GEMM on the sm_100a tensor cores (tcgen05 / UMMA) for the
-// surrogate network: C[M][N] = sum_k A[M][k] B[N][k] (both operands
-// K-major, BF16; FP32 accumulation in tensor memory) with fused epilogues.
+// surrogate network's weight gradients: C[M][N] = sum_k A[M][k] B[N][k] (both
+// operands K-major, BF16; FP32 accumulation in tensor memory), written
+// transposed as FP32 split-K partials.  The PTX helpers here are shared with
+// the fused forward / input-gradient kernel (mlp_chain.cuh).
 //
 // One CTA (8 warps) computes a 128 x 64 tile over a K range of at most 256:
 //   * thread 0 issues every TMA load of the range at once (64-wide K chunks,
@@ -8,9 +10,7 @@
 //   * one lane of warp 1 issues tcgen05.mma (M=128, N=64, K=16) per 16-wide
 //     slice as each chunk lands, then tcgen05.commit to the "done" barrier;
 //   * all eight warps read accumulator rows with tcgen05.ld (warp w: lanes
-//     32 (w % 4) .. + 31, the column half w / 4) and apply the epilogue.
-// The 64-wide N tile gives the small surrogate GEMMs (N = 256) four column
-// tiles, so 128 CTAs share the epilogue work instead of 64.
+//     32 (w % 4) .. + 31, the column half w / 4) and store them.
 // Every mbarrier wait is bounded: on expiry the CTA records an error flag,
 // waits (bounded) for its own copies, frees its tensor memory and returns.
 #pragma once
@@ -32,29 +32,12 @@ constexpr int kSmemBytes = kMaxChunks * (kStageA + kStageB) + 1024 /* align */ +
 static_assert(kBN % 64 == 0, "two column halves of whole 32-column groups");
 constexpr long kSpinLimit = 1L << 20;
 
-enum Epilogue {
-    kEpiF32 = 0,      // out_f32[z][n][m] = acc (split-K partials, transposed)
-    kEpiFwdGelu = 1,  // z = acc + bias -> out_f32 [n][m]; gelu(z) -> out_bf [m][n] and out_bfT [n][m]
-    kEpiFwdOut = 2,   // y = acc + bias -> out_f32 [n][m]; with a target [n][m]: loss gradient -> out_bf / out_bfT
-    kEpiBwdGelu = 3,  // dz = acc * gelu'(zin [n][m]) -> out_bf / out_bfT
-};
-
 struct GemmArgs {
     int M, N, K;          // logical sizes (rows of A, rows of B, reduction)
     int k_split;          // K range per blockIdx.z (multiple of 64, <= 256)
-    const float *bias;    // [N]
-    // FP32 outputs and inputs are stored transposed ([N][M]): the epilogue
-    // thread owns one row m, so consecutive lanes touch consecutive addresses
-    float *out_f32;       // kEpiF32: [splits][N][M]; kEpiFwdGelu: z [N][M]; kEpiFwdOut: y [N][M]
-    __nv_bfloat16 *out_bf;   // [M][N]
-    __nv_bfloat16 *out_bfT;  // [N][M]
-    const float *zin;     // kEpiBwdGelu: pre-activation [N][M]
-    const float *target;  // kEpiFwdOut: [N][M] or null (inference)
-    const float *tweight; // [N] loss weight per output
-    int m_valid;          // rows that count in the loss
-    int n_valid;          // outputs that count in the loss
-    float grad_scale;     // d loss / d y = grad_scale * w (y - t)
-    float *loss_part;     // [grid x * grid y] sum w (y - t)^2 per CTA
+    // split-K partials stored transposed, [splits][N][M]: the epilogue thread
+    // owns one row m, so consecutive lanes touch consecutive addresses
+    float *out_f32;
     unsigned *err;
 };
 
@@ -146,7 +129,6 @@ __device__ __forceinline__ float gelu_grad(float z) {
 }
 
 // ----------------------------------------------------------------- kernel
-template <int EPI>
 __global__ void __launch_bounds__(kThreads, 1)
     k_umma_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmArgs g) {
     extern __shared__ unsigned char smem_raw[];
@@ -157,8 +139,6 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + kMaxChunks * (kStageA + kStageB));
     uint64_t *done = full + kMaxChunks;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
-    __shared__ float red[kThreads / 32];
-    __shared__ float stage[kThreads / 32][32][33];  // per-warp 32 x 32 tile, padded against bank conflicts
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
@@ -208,9 +188,6 @@ __global__ void __launch_bounds__(kThreads, 1)
 
     const int quad = warp & 3, half = warp >> 2;
     const int m = m0 + quad * 32 + lane;
-    const bool mrow = m < g.M;
-    float loss = 0.f;
-    float(*st)[33] = stage[warp];
     if (have) {
 #pragma unroll 1
         for (int cc = half * (kBN / 64); cc < (half + 1) * (kBN / 64); cc++) {
@@ -221,67 +198,15 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
             for (int j = 0; j < 32; j++) {
                 const int n = nb + j;
-                const bool ok = mrow && n < g.N;
-                const size_t nm = (size_t)n * g.M + m;
-                float r = 0.f;  // value of the row-major BF16 output
-                if (EPI == kEpiF32) {
-                    if (ok) g.out_f32[(size_t)blockIdx.z * g.M * g.N + nm] = v[j];
-                } else if (EPI == kEpiFwdGelu) {
-                    if (ok) {
-                        const float z = v[j] + g.bias[n];
-                        g.out_f32[nm] = z;
-                        r = gelu(z);
-                        g.out_bfT[nm] = __float2bfloat16_rn(r);
-                    }
-                } else if (EPI == kEpiFwdOut) {
-                    if (ok) {
-                        const float y = v[j] + g.bias[n];
-                        g.out_f32[nm] = y;
-                        if (g.target) {
-                            if (n < g.n_valid && m < g.m_valid) {
-                                const float e = y - g.target[nm];
-                                loss += g.tweight[n] * e * e;
-                                r = g.grad_scale * g.tweight[n] * e;
-                            }
-                            g.out_bfT[nm] = __float2bfloat16_rn(r);
-                        }
-                    }
-                } else {  // kEpiBwdGelu
-                    if (ok) {
-                        r = v[j] * gelu_grad(g.zin[nm]);
-                        g.out_bfT[nm] = __float2bfloat16_rn(r);
-                    }
-                }
-                st[lane][j] = r;
-            }
-            // row-major BF16 output [m][n]: through the padded tile, one row per
-            // instruction (lane = column)
-            const bool rowmajor = EPI == kEpiFwdGelu || EPI == kEpiBwdGelu || (EPI == kEpiFwdOut && g.target);
-            if (rowmajor) {
-                __syncwarp();
-                const int n = nb + lane;
-#pragma unroll 4
-                for (int rr = 0; rr < 32; rr++) {
-                    const int mr = m0 + quad * 32 + rr;
-                    if (mr < g.M && n < g.N) g.out_bf[(size_t)mr * g.N + n] = __float2bfloat16_rn(st[rr][lane]);
-                }
-                __syncwarp();
+                if (m < g.M && n < g.N) g.out_f32[(size_t)blockIdx.z * g.M * g.N + (size_t)n * g.M + m] = v[j];
             }
         }
     } else if (threadIdx.x == 0) {
         // bounded wait for this CTA's own copies before its memory goes away
         for (int c = 0; c < nk; c++) mbar_wait(&full[c], 0, g.err, 4u);
     }
-    if (EPI == kEpiFwdOut && g.target && g.loss_part) {
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) loss += __shfl_down_sync(0xffffffffu, loss, off);
-        if (lane == 0) red[warp] = loss;
-    }
     tc_fence_before();
     __syncthreads();
-    if (EPI == kEpiFwdOut && g.target && g.loss_part && threadIdx.x == 0)
-        g.loss_part[blockIdx.x * gridDim.y + blockIdx.y] =
-            ((red[0] + red[1]) + (red[2] + red[3])) + ((red[4] + red[5]) + (red[6] + red[7]));
     if (warp == 0) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kBN));
