@@ -170,48 +170,71 @@ __global__ void k_bias_grads(const __grid_constant__ BiasGradArgs a) {
 struct AdamArgs {
     float lr, b1, b2, eps;
     const long long *step;  // number of updates so far (incremented by the caller's counter kernel)
-    const float *corr;      // [2]: 1 - b1^t and 1 - b2^t of this update (k_adam_prep)
 };
-// the bias-correction denominators of update t = step + 1, once per step
-__global__ void k_adam_prep(AdamArgs a, float *corr) {
-    const float t = (float)(*a.step + 1);
-    corr[0] = 1.f - powf(a.b1, t);
-    corr[1] = 1.f - powf(a.b2, t);
-}
-
-// Adam on one weight matrix (gradient = sum of the split partials, stored
-// [splits][K][N] by the weight-gradient GEMM) in [k][n] order: the FP32
-// master weights and the moments are kept in that order too, so every FP32
-// access is coalesced; writes the BF16 copies W [N][K] and W^T [K][N].
-__global__ void k_adam(float *w, float *m1, float *m2, const float *part, int splits, int N, int K, int n_live,
-                       int k_live, __nv_bfloat16 *wb, __nv_bfloat16 *wbt, AdamArgs a) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // [k][n] order
-    if (i >= (size_t)N * K) return;
-    const int k = (int)(i / N), n = (int)(i % N);
-    float gsum = 0.f;
-    for (int s = 0; s < splits; s++) gsum += part[(size_t)s * N * K + i];
-    float wv = w[i];
-    if (n < n_live && k < k_live) {
-        const float mm = a.b1 * m1[i] + (1.f - a.b1) * gsum;
-        const float vv = a.b2 * m2[i] + (1.f - a.b2) * gsum * gsum;
-        m1[i] = mm;
-        m2[i] = vv;
-        const float mh = mm / a.corr[0], vh = vv / a.corr[1];
-        wv -= a.lr * mh / (sqrtf(vh) + a.eps);
-        w[i] = wv;
+// Every layer's weights and biases in one launch: element i of the table
+// (weights of layer 0, 1, ... then biases of layer 0, 1, ...).  Weights are
+// updated in [k][n] order (the gradient is the sum of the split partials,
+// stored [splits][K][N] by the weight-gradient GEMM); the FP32 master weights
+// and the moments are kept in that order too, so every FP32 access is
+// coalesced.  Writes the BF16 copies W [N][K] and W^T [K][N].  The
+// bias-correction denominators 1 - b^t are computed once per block.
+struct AdamTable {
+    float *w[umma::kChainMaxLayers], *wm[umma::kChainMaxLayers], *wv[umma::kChainMaxLayers];
+    const float *part[umma::kChainMaxLayers];
+    __nv_bfloat16 *wb[umma::kChainMaxLayers], *wbt[umma::kChainMaxLayers];
+    float *b[umma::kChainMaxLayers], *bm[umma::kChainMaxLayers], *bv[umma::kChainMaxLayers];
+    const float *db[umma::kChainMaxLayers];
+    int N[umma::kChainMaxLayers], K[umma::kChainMaxLayers];
+    int n_live[umma::kChainMaxLayers], k_live[umma::kChainMaxLayers];
+    long long first_w[umma::kChainMaxLayers + 1];  // prefix of N K over the layers
+    int first_b[umma::kChainMaxLayers + 1];        // prefix of N over the layers
+    int L, splits;
+};
+__global__ void k_adam_all(const __grid_constant__ AdamTable t, AdamArgs a) {
+    __shared__ float corr[2];
+    if (threadIdx.x == 0) {
+        const float tt = (float)(*a.step + 1);
+        corr[0] = 1.f - powf(a.b1, tt);
+        corr[1] = 1.f - powf(a.b2, tt);
     }
-    const __nv_bfloat16 b = __float2bfloat16_rn(wv);
-    wb[(size_t)n * K + k] = b;
-    wbt[i] = b;
-}
-__global__ void k_adam_bias(float *b, float *m1, float *m2, const float *g, int N, int n_live, AdamArgs a) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= N || n >= n_live) return;
-    const float mm = a.b1 * m1[n] + (1.f - a.b1) * g[n];
-    const float vv = a.b2 * m2[n] + (1.f - a.b2) * g[n] * g[n];
-    m1[n] = mm;
-    m2[n] = vv;
-    b[n] -= a.lr * (mm / a.corr[0]) / (sqrtf(vv / a.corr[1]) + a.eps);
+    __syncthreads();
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nw = t.first_w[t.L];
+    if (e < nw) {
+        int l = 0;
+        while (l + 1 < t.L && e >= t.first_w[l + 1]) l++;
+        const size_t i = (size_t)(e - t.first_w[l]);  // [k][n] order
+        const int N = t.N[l], K = t.K[l];
+        const int k = (int)(i / N), n = (int)(i % N);
+        float gsum = 0.f;
+        for (int s = 0; s < t.splits; s++) gsum += t.part[l][(size_t)s * N * K + i];
+        float wv = t.w[l][i];
+        if (n < t.n_live[l] && k < t.k_live[l]) {
+            const float mm = a.b1 * t.wm[l][i] + (1.f - a.b1) * gsum;
+            const float vv = a.b2 * t.wv[l][i] + (1.f - a.b2) * gsum * gsum;
+            t.wm[l][i] = mm;
+            t.wv[l][i] = vv;
+            const float mh = mm / corr[0], vh = vv / corr[1];
+            wv -= a.lr * mh / (sqrtf(vh) + a.eps);
+            t.w[l][i] = wv;
+        }
+        const __nv_bfloat16 bv = __float2bfloat16_rn(wv);
+        t.wb[l][(size_t)n * K + k] = bv;
+        t.wbt[l][i] = bv;
+        return;
+    }
+    const long long j = e - nw;
+    if (j >= t.first_b[t.L]) return;
+    int l = 0;
+    while (l + 1 < t.L && j >= t.first_b[l + 1]) l++;
+    const int n = (int)(j - t.first_b[l]);
+    if (n >= t.n_live[l]) return;
+    const float g = t.db[l][n];
+    const float mm = a.b1 * t.bm[l][n] + (1.f - a.b1) * g;
+    const float vv = a.b2 * t.bv[l][n] + (1.f - a.b2) * g * g;
+    t.bm[l][n] = mm;
+    t.bv[l][n] = vv;
+    t.b[l][n] -= a.lr * (mm / corr[0]) / (sqrtf(vv / corr[1]) + a.eps);
 }
 __global__ void k_count(long long *step) { *step += 1; }
 // BF16 copies W [N][K] and W^T [K][N] of the FP32 master weights (kept [K][N])
@@ -249,7 +272,6 @@ struct bd_surrogate {
     std::vector<float *> db;          // bias gradients
     float *loss_part = nullptr;
     long long *step = nullptr;
-    float *corr = nullptr;            // Adam bias-correction denominators of the current update
     unsigned *err = nullptr;
     float *data_x = nullptr, *data_y = nullptr;
     int n_data = 0;
@@ -284,7 +306,7 @@ void free_surrogate(bd_surrogate *s) {
     for (auto *p : s->z) F(p);
     for (auto *p : s->dzt) F(p);
     for (auto *p : s->db) F(p);
-    F(s->x0); F(s->y); F(s->t); F(s->tw); F(s->part); F(s->loss_part); F(s->step); F(s->corr); F(s->err); F(s->data_x);
+    F(s->x0); F(s->y); F(s->t); F(s->tw); F(s->part); F(s->loss_part); F(s->step); F(s->err); F(s->data_x);
     F(s->data_y);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -390,17 +412,31 @@ int backward(bd_surrogate *s) {
 }
 
 int adam(bd_surrogate *s) {
-    AdamArgs a{s->lr, 0.9f, 0.999f, 1e-8f, s->step, s->corr};
-    k_adam_prep<<<1, 1, 0, s->stream>>>(a, s->corr);
-    const int splits = s->batch / s->ksplit;
+    AdamArgs a{s->lr, 0.9f, 0.999f, 1e-8f, s->step};
+    AdamTable t;
+    std::memset(&t, 0, sizeof(t));
+    t.L = s->L;
+    t.splits = s->batch / s->ksplit;
     for (int l = 0; l < s->L; l++) {
-        const size_t n = (size_t)s->Np[l] * s->Kp[l];
-        k_adam<<<div_up((long)n, 256), 256, 0, s->stream>>>(s->w[l], s->wm[l], s->wv[l], s->part + part_offset(s, l),
-                                                             splits, s->Np[l], s->Kp[l], s->Nl[l], s->Kl[l], s->wb[l],
-                                                             s->wbt[l], a);
-        k_adam_bias<<<div_up(s->Np[l], 128), 128, 0, s->stream>>>(s->b[l], s->bm[l], s->bv[l], s->db[l], s->Np[l],
-                                                                  s->Nl[l], a);
+        t.w[l] = s->w[l];
+        t.wm[l] = s->wm[l];
+        t.wv[l] = s->wv[l];
+        t.part[l] = s->part + part_offset(s, l);
+        t.wb[l] = s->wb[l];
+        t.wbt[l] = s->wbt[l];
+        t.b[l] = s->b[l];
+        t.bm[l] = s->bm[l];
+        t.bv[l] = s->bv[l];
+        t.db[l] = s->db[l];
+        t.N[l] = s->Np[l];
+        t.K[l] = s->Kp[l];
+        t.n_live[l] = s->Nl[l];
+        t.k_live[l] = s->Kl[l];
+        t.first_w[l + 1] = t.first_w[l] + (long long)s->Np[l] * s->Kp[l];
+        t.first_b[l + 1] = t.first_b[l] + s->Np[l];
     }
+    const long long total = t.first_w[s->L] + t.first_b[s->L];
+    k_adam_all<<<(unsigned)div_up(total, 256), 256, 0, s->stream>>>(t, a);
     k_count<<<1, 1, 0, s->stream>>>(s->step);
     BD_LAUNCH_CHECK();
     return BD_OK;
@@ -480,7 +516,6 @@ int bd_surrogate_create(int n_in, int n_out, int width, int depth, int batch, un
     s->loss_cells = (batch / kBM) * umma::kChainCluster;
     A((void **)&s->loss_part, (size_t)s->loss_cells * 4);
     A((void **)&s->step, sizeof(long long));
-    A((void **)&s->corr, 2 * sizeof(float));
     A((void **)&s->err, sizeof(unsigned));
     if (!ok) {
         free_surrogate(s);
