@@ -14,10 +14,16 @@
 // GEMMs, of W_l^T for the backward ones) comes by TMA (no multicast); the
 // accumulator is 128 lanes x N / 4 columns of tensor memory.  The epilogue of
 // each GEMM writes its slice of the next GEMM's A operand into the other
-// buffer of all four CTAs (distributed shared memory stores), and the
-// transposed copies the weight-gradient GEMMs need (H_l^T, dZ_l^T, both
-// [N][M], lane = row so stores coalesce) plus Z_l to global memory; one
-// cluster barrier per GEMM then publishes the new A operand.  The
+// buffer of all four CTAs, and the transposed copies the weight-gradient
+// GEMMs need (H_l^T, dZ_l^T, both [N][M], lane = row so stores coalesce) plus
+// Z_l to global memory.  When N = 256 a CTA's slice is one whole 16 KB chunk
+// of the A operand: the epilogue writes it locally and one thread copies it
+// to the three peers with shared-to-shared bulk copies that complete on the
+// peer's mbarrier.  A peer's buffer is free by then: the copy follows this
+// CTA's MMA, which needed the peer's slice of the current operand, which the
+// peer sent after its own MMA of the previous GEMM had read the buffer.
+// Other shapes use per-thread distributed shared-memory stores and one
+// cluster barrier per GEMM.  The
 // weight-gradient GEMMs reduce over the batch and stay separate launches.
 // The next GEMM's weights are loaded while the epilogue of the current one
 // runs.  Every mbarrier wait is bounded: on expiry the CTA records an error
@@ -124,6 +130,17 @@ __device__ __forceinline__ void chain_put8_cluster(uint32_t a, const float *v) {
                      : "memory");
     }
 }
+// Eight values as BF16 into this CTA's A buffer (`a` points at their unit).
+__device__ __forceinline__ void chain_put8_local(unsigned char *a, const float *v) {
+    __nv_bfloat162 p0 = __floats2bfloat162_rn(v[0], v[1]), p1 = __floats2bfloat162_rn(v[2], v[3]);
+    __nv_bfloat162 p2 = __floats2bfloat162_rn(v[4], v[5]), p3 = __floats2bfloat162_rn(v[6], v[7]);
+    uint4 q;
+    q.x = *reinterpret_cast<uint32_t *>(&p0);
+    q.y = *reinterpret_cast<uint32_t *>(&p1);
+    q.z = *reinterpret_cast<uint32_t *>(&p2);
+    q.w = *reinterpret_cast<uint32_t *>(&p3);
+    *reinterpret_cast<uint4 *>(a) = q;
+}
 __device__ __forceinline__ void cluster_sync_all() {
     asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
@@ -154,7 +171,8 @@ __global__ void __launch_bounds__(kChainThreads, 1)
     uint64_t *bar_x = reinterpret_cast<uint64_t *>(smem + 2 * kChainA + kChainB);  // X0 landed
     uint64_t *bar_b = bar_x + 1;             // B of the current GEMM landed (one phase per GEMM)
     uint64_t *bar_d = bar_x + 2;             // MMAs of the current GEMM completed (one phase per GEMM)
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar_x + 3);
+    uint64_t *bar_a = bar_x + 3;             // [2]: the peers' chunks of A buffer b landed (bulk copies)
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar_x + 5);
     __shared__ float red[kChainThreads / 32];
     __shared__ float s_bias[kChainMaxNc], s_tw[kChainMaxNc];  // per-column epilogue inputs of the GEMM
 
@@ -172,6 +190,8 @@ __global__ void __launch_bounds__(kChainThreads, 1)
         mbar_init(bar_x, 1);
         mbar_init(bar_b, 1);
         mbar_init(bar_d, 1);
+        mbar_init(&bar_a[0], 1);
+        mbar_init(&bar_a[1], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
@@ -204,7 +224,9 @@ __global__ void __launch_bounds__(kChainThreads, 1)
         load_b(0);
     }
 
-    bool failed = false;  // uniform over the CTA
+    bool failed = false;   // uniform over the CTA
+    bool bulk_in = false;  // this GEMM's A operand came from the peers by bulk copy
+    int na0 = 0, na1 = 0;  // bulk-filled uses of A buffers 0 and 1 (bar_a phases)
     float loss = 0.f;
     for (int gi = 0; gi < nG; gi++) {
         const ChainStep c = chain_step(g, gi);
@@ -216,6 +238,7 @@ __global__ void __launch_bounds__(kChainThreads, 1)
         if (warp == 1 && lane == 0) {  // one thread issues the MMAs of the GEMM
             bool go = !failed && (gi > 0 || mbar_wait(bar_x, 0, g.err, 1u));
             go = go && mbar_wait(bar_b, ph, g.err, 1u);
+            go = go && (!bulk_in || mbar_wait(&bar_a[gi & 1], (uint32_t)(((gi & 1) ? na1 : na0) & 1), g.err, 3u));
             issued = go;
             if (go) {
                 tc_fence_after();
@@ -232,6 +255,10 @@ __global__ void __launch_bounds__(kChainThreads, 1)
             umma_commit(bar_d);  // arrives when every MMA issued so far has completed
         }
         __syncwarp();
+        if (bulk_in) {
+            if (gi & 1) na1++;
+            else na0++;
+        }
         // the epilogue's inputs that do not depend on the MMAs load under them:
         // per-column bias and loss weight to shared memory, per-element Z_{l-1}
         // (backward) or targets (output layer) to registers
@@ -250,11 +277,18 @@ __global__ void __launch_bounds__(kChainThreads, 1)
         }
         const bool done = mbar_wait(bar_d, ph, g.err, 2u) && issued;  // the commit arrives even when nothing was issued
         tc_fence_after();
+        // this CTA's earlier bulk copies have read their source (the A buffer
+        // this epilogue writes was the source two GEMMs ago)
+        if (tid == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
         const bool ok = __syncthreads_and(done) != 0;
         failed = failed || !ok;
         // the B buffer is free: the next GEMM's weights load under this epilogue
         if (tid == 0 && gi + 1 < nG && !failed) load_b(gi + 1);
         const bool next_a = gi + 1 < nG;  // a GEMM follows that reads the A operand written here
+        // a CTA's columns of an N = 256 GEMM are one whole 16 KB chunk of the next
+        // A operand: written locally, then bulk-copied to the three peers;
+        // otherwise every thread stores its values into all four CTAs
+        const bool bulk_next = next_a && nc == kBK;
         const uint32_t trow = tmem + ((uint32_t)(quad * 32) << 16);
         if (ok) {  // warp (quad, half): rows 32 quad .. + 31 (lane = row), half of the CTA's columns
             float v[32];
@@ -322,14 +356,39 @@ __global__ void __launch_bounds__(kChainThreads, 1)
             if (next_a)
 #pragma unroll
                 for (int u = 0; u < 4; u++)
-                    if (u * 8 < cw) chain_put8_cluster(a_next + chain_a_offset(r, nbase + 8 * u), v + 8 * u);
+                    if (u * 8 < cw) {
+                        if (bulk_next) chain_put8_local(sA0 + ((gi + 1) & 1) * kChainA + chain_a_offset(r, nbase + 8 * u), v + 8 * u);
+                        else chain_put8_cluster(a_next + chain_a_offset(r, nbase + 8 * u), v + 8 * u);
+                    }
         }
-        // publish the next A operand to the cluster (and free this one)
-        asm volatile("fence.proxy.async.shared::cluster;" ::: "memory");
+        // publish the next A operand: the chunk by bulk copy under the peers'
+        // mbarriers, or the stores by a cluster barrier (which also frees this one)
+        if (bulk_next) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        else asm volatile("fence.proxy.async.shared::cluster;" ::: "memory");
         tc_fence_before();
-        cluster_sync_all();
+        if (bulk_next) __syncthreads();
+        else cluster_sync_all();
         tc_fence_after();
+        if (bulk_next && tid == 0 && !failed) {
+            uint64_t *ba = &bar_a[(gi + 1) & 1];
+            mbar_expect_tx(ba, (uint32_t)((kChainCluster - 1) * kBM * 128));  // the peers' chunks
+            const uint32_t src = a_next + q * (uint32_t)(kBM * 128);
+            for (int p = 1; p < kChainCluster; p++) {
+                const uint32_t dq = (q + (uint32_t)p) % kChainCluster;
+                uint32_t dst, mb;
+                asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(dst) : "r"(src), "r"(dq));
+                asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(mb) : "r"(smem_u32(ba)), "r"(dq));
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                    "r"(src), "r"((uint32_t)(kBM * 128)), "r"(mb)
+                    : "memory");
+            }
+            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        }
+        bulk_in = bulk_next;
     }
+    if (tid == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");  // sources read
+    cluster_sync_all();  // no shared-memory traffic between the CTAs is left when any of them exits
     if (failed && tid == 0) {  // bounded wait for this CTA's own copies before its memory goes away
         mbar_wait(bar_x, 0, g.err, 4u);
         if (nb > 0) mbar_wait(bar_b, (uint32_t)((nb - 1) & 1), g.err, 4u);
