@@ -243,6 +243,13 @@ int configure_kernels(bd_engine *e) {
 #undef BD_ATTR
     if (cudaFuncSetAttribute(k_list_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e->lsmem) != cudaSuccess)
         rc = 1;
+    if (e->lrep_smem > 0) {  // variant 5 rebuilds from shared memory
+        if (cudaFuncSetAttribute(k_list_replica<false, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)e->lrep_smem) != cudaSuccess ||
+            cudaFuncSetAttribute(k_list_replica<true, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)e->lrep_smem) != cudaSuccess)
+            rc = 1;
+    }
     return rc ? BD_ERR_CUDA : BD_OK;
 }
 
@@ -357,10 +364,12 @@ template <int V>
 int launch_list_replica_v(bd_engine *e, int cur, int nsteps) {
     constexpr int T = ListVariant<V>::kThreads;
     const ListArgs a = make_largs(e, cur);
+    const bool shared_build = V == 5 && e->lrep_smem > 0;
     const ListPersist lp{{e->lpos[0], e->lpos[1]}, cur & 1, e->cnt[0], e->pos[0], e->cap, e->nbr, e->nnb,
-                         e->pbuild, e->d_rep_order, e->d_builds, e->d_step_rebuilt};
-    if (e->extra_pot) k_list_replica<true, V><<<e->R, T, 0, e->stream>>>(a, lp, e->d_ni, nsteps);
-    else k_list_replica<false, V><<<e->R, T, 0, e->stream>>>(a, lp, e->d_ni, nsteps);
+                         e->pbuild, e->d_rep_order, e->d_builds, e->d_step_rebuilt, shared_build ? 1 : 0};
+    const size_t sm = shared_build ? e->lrep_smem : 0;
+    if (e->extra_pot) k_list_replica<true, V><<<e->R, T, sm, e->stream>>>(a, lp, e->d_ni, nsteps);
+    else k_list_replica<false, V><<<e->R, T, sm, e->stream>>>(a, lp, e->d_ni, nsteps);
     BD_LAUNCH_CHECK();
     k_list_replica_done<<<1, 256, 0, e->stream>>>(e->lflag, e->R, e->d_step_rebuilt, nsteps, e->d_builds);
     BD_LAUNCH_CHECK();
@@ -765,6 +774,12 @@ int bd_engine_create(const bd_system_desc *systems, int nsys, const bd_engine_op
             std::stable_sort(order.begin(), order.end(),
                              [&](int a, int b) { return e->sysh[a].n > e->sysh[b].n; });
             cudaMemcpyAsync(e->d_rep_order, order.data(), sizeof(int) * e->R, cudaMemcpyHostToDevice, e->stream);
+            size_t need = 0;  // the largest in-block rebuild from shared memory
+            for (int r = 0; r < e->R; r++) {
+                const SysDev &S = e->sysh[r];
+                need = std::max(need, replica_shared_build_bytes(S.n, S.ncell * S.ncell * S.ncell));
+            }
+            e->lrep_smem = need <= (size_t)227 * 1024 ? need : 0;
             cudaStreamSynchronize(e->stream);  // the host vector goes out of scope
         }
         const int one = 1;

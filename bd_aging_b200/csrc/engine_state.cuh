@@ -83,6 +83,7 @@ struct bd_engine {
     int *img = nullptr;             // [3][P] face crossings since the origin (displacement on demand)
     float *amp_tab = nullptr;       // [graph_steps][R][2] noise amplitudes of a launch batch
     int *d_rep_order = nullptr;     // per-replica launch (variants 3-5): replica of each block
+    size_t lrep_smem = 0;           // variant 5: shared memory of an in-block rebuild (0: from global memory)
     int *d_step_rebuilt = nullptr;  // [graph_steps] steps of such a launch that rebuilt a replica
     // set_positions scratch (storage order computed on the device)
     float *ld_in = nullptr;        // [P][3] positions as given

@@ -624,6 +624,7 @@ struct ListPersist {
     const int *order;      // replica of each block, most particles first
     long long *builds;     // [0] replica list builds, [1] steps that rebuilt
     int *step_rebuilt;     // [step of the launch]: some replica rebuilt before it
+    int shared_build;      // variant 5: rebuild from shared memory (replica_rebuild_shared)
 };
 
 // cell of a by-id position, as bin_particle and the step kernels bin it
@@ -641,10 +642,34 @@ __device__ __forceinline__ int wrap_cell(int g, int nc, float L, float &shift) {
     return g;
 }
 
-// List of particle sid from the sorted buckets of its replica.
-__device__ __forceinline__ void replica_list(const ListArgs &a, const ListPersist &lp, const SysDev &S, int sid) {
+// A replica's cells for the in-block list build, each in storage-id order:
+// the bucket buffer in global memory (cap slots per cell), or a compact
+// cell-sorted copy in shared memory.
+struct CellsGlobal {
+    const int *cnt;
+    const float4 *bucket;
+    int cap, cell_base;
+    __device__ __forceinline__ const float4 *cell(int c, int &m) const {
+        const int gc = cell_base + c;
+        m = min(cnt[gc], cap);
+        return bucket + (size_t)gc * cap;
+    }
+};
+struct CellsShared {
+    const int *start;  // [cells + 1]
+    const float4 *pos;
+    __device__ __forceinline__ const float4 *cell(int c, int &m) const {
+        m = start[c + 1] - start[c];
+        return pos + start[c];
+    }
+};
+
+// List of particle sid from the sorted cells of its replica.
+template <class CELLS>
+__device__ __forceinline__ void replica_list(const ListArgs &a, const ListPersist &lp, const SysDev &S, int sid,
+                                             const CELLS &cells) {
     const float4 v = a.pos_in[sid];
-    const int np = a.np, nc = S.ncell, cap = lp.cap;
+    const int np = a.np, nc = S.ncell;
     const int tm = (int)(__float_as_uint(v.w) >> 31);
     const float cut_b = S.lcut2[tm], cut_s = S.lcut2[tm + 1];  // towards a big / a small partner
     const float L = S.L;
@@ -659,9 +684,8 @@ __device__ __forceinline__ void replica_list(const ListArgs &a, const ListPersis
             for (int dx = -1; dx <= 1; dx++) {
                 float shx;
                 const int gx = wrap_cell(c.x + dx, nc, L, shx);
-                const int gc = S.cell_base + gx + nc * (gy + nc * gz);
-                const int m = min(lp.cnt[gc], cap);
-                const float4 *b = lp.bucket + (size_t)gc * cap;
+                int m;
+                const float4 *b = cells.cell(gx + nc * (gy + nc * gz), m);
                 for (int k = 0; k < m; k++) {
                     const float4 q = b[k];
                     const unsigned wq = __float_as_uint(q.w);
@@ -717,7 +741,95 @@ __device__ __forceinline__ void replica_rebuild(const ListArgs &a, const ListPer
         }
     }
     __syncthreads();
-    for (int sid = base + tid; sid < end; sid += T) replica_list(a, lp, S, sid);
+    const CellsGlobal cells{lp.cnt, lp.bucket, cap, cb};
+    for (int sid = base + tid; sid < end; sid += T) replica_list(a, lp, S, sid, cells);
+    __syncthreads();
+}
+
+// Shared-memory bytes of the in-block rebuild from shared memory for a
+// replica of n particles in c cells: exclusive cell starts [c + 1] and fill
+// counters [c], then the positions sorted by cell.
+__host__ __device__ inline size_t replica_shared_build_bytes(int n, int c) {
+    return (((size_t)(2 * c + 1) * 4 + 15) & ~(size_t)15) + (size_t)n * 16;
+}
+
+// The same lists as replica_rebuild, from a compact copy of the replica
+// sorted by cell (a counting sort, then each cell by storage id) in the
+// block's dynamic shared memory `dsm` (replica_shared_build_bytes).  Cells
+// above the bucket capacity raise the overflow status as the bucket build
+// does.
+__device__ __forceinline__ void replica_rebuild_shared(const ListArgs &a, const ListPersist &lp, const SysDev &S,
+                                                       unsigned char *dsm) {
+    const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    const int nc = S.ncell, ncell = nc * nc * nc;
+    const int base = S.part_base, n = S.n;
+    int *s_start = reinterpret_cast<int *>(dsm);  // [ncell + 1]
+    int *s_fill = s_start + ncell + 1;            // [ncell]
+    float4 *s_pos = reinterpret_cast<float4 *>(dsm + (((size_t)(2 * ncell + 1) * 4 + 15) & ~(size_t)15));
+    __shared__ int s_warp[32];
+    for (int c = tid; c < ncell; c += T) s_fill[c] = 0;
+    __syncthreads();
+    for (int i = tid; i < n; i += T) {
+        const int3 c = list_cell_of(a.pos_in[base + i], S);
+        atomicAdd(&s_fill[c.x + nc * (c.y + nc * c.z)], 1);
+    }
+    __syncthreads();
+    // exclusive scan of the counts: a segment per thread, then the warps
+    const int per = (ncell + T - 1) / T, c0 = min(tid * per, ncell), c1 = min(c0 + per, ncell);
+    int local = 0;
+    for (int c = c0; c < c1; c++) local += s_fill[c];
+    int incl = local;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += y;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        int w = lane < (T >> 5) ? s_warp[lane] : 0;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, w, off);
+            if (lane >= off) w += y;
+        }
+        s_warp[lane] = w;
+    }
+    __syncthreads();
+    int run = incl - local + (warp > 0 ? s_warp[warp - 1] : 0);
+    for (int c = c0; c < c1; c++) {
+        const int k = s_fill[c];
+        if (k > lp.cap) set_status(a.status, kStatCellOverflow);
+        s_start[c] = run;
+        s_fill[c] = run;
+        run += k;
+    }
+    if (tid == 0) s_start[ncell] = n;
+    __syncthreads();
+    for (int i = tid; i < n; i += T) {
+        const float4 v = a.pos_in[base + i];
+        const int3 c = list_cell_of(v, S);
+        s_pos[atomicAdd(&s_fill[c.x + nc * (c.y + nc * c.z)], 1)] = v;
+    }
+    __syncthreads();
+    // each cell in storage-id order (insertion sort, a thread per cell)
+    for (int c = tid; c < ncell; c += T) {
+        float4 *b = s_pos + s_start[c];
+        const int m = s_start[c + 1] - s_start[c];
+        for (int i = 1; i < m; i++) {
+            const float4 v = b[i];
+            const unsigned key = __float_as_uint(v.w) & 0x7fffffffu;
+            int j = i - 1;
+            while (j >= 0 && (__float_as_uint(b[j].w) & 0x7fffffffu) > key) {
+                b[j + 1] = b[j];
+                j--;
+            }
+            b[j + 1] = v;
+        }
+    }
+    __syncthreads();
+    const CellsShared cells{s_start, s_pos};
+    for (int sid = base + tid; sid < base + n; sid += T) replica_list(a, lp, S, sid, cells);
     __syncthreads();
 }
 
@@ -727,6 +839,7 @@ __device__ __forceinline__ void replica_rebuild(const ListArgs &a, const ListPer
 template <bool EXTRA, int V>
 __global__ void __launch_bounds__(ListVariant<V>::kThreads, ListVariant<V>::kMinBlocks)
     k_list_replica(ListArgs a, ListPersist lp, const long long *ni_base, int nsteps) {
+    extern __shared__ __align__(16) unsigned char dsm[];
     const int rep = lp.order[blockIdx.x];
     const SysDev &S = a.sys[rep];
     const int base = S.part_base, end = S.part_base + S.n;
@@ -738,7 +851,14 @@ __global__ void __launch_bounds__(ListVariant<V>::kThreads, ListVariant<V>::kMin
         as.pos_in = odd ? lp.pos[1] : lp.pos[0];
         as.pos_out = odd ? lp.pos[0] : lp.pos[1];
         if (need) {
-            replica_rebuild(as, lp, S);
+            bool done = false;
+            if constexpr (V == 5) {
+                if (lp.shared_build) {
+                    replica_rebuild_shared(as, lp, S, dsm);
+                    done = true;
+                }
+            }
+            if (!done) replica_rebuild(as, lp, S);
             if (threadIdx.x == 0) {
                 atomicAdd((unsigned long long *)lp.builds, 1ull);
                 lp.step_rebuilt[s] = 1;
