@@ -835,7 +835,7 @@ __device__ __forceinline__ void replica_rebuild_shared(const ListArgs &a, const 
 
 // nsteps steps of replica order[blockIdx.x] (Philox noise; nsteps at most the
 // amplitude table's batch).  The replica's flag on entry asks for a rebuild
-// before the first step; on exit it holds the last step's verdict.
+// before the first step; on exit it holds the last step's decision.
 template <bool EXTRA, int V>
 __global__ void __launch_bounds__(ListVariant<V>::kThreads, ListVariant<V>::kMinBlocks)
     k_list_replica(ListArgs a, ListPersist lp, const long long *ni_base, int nsteps) {

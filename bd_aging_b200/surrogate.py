@@ -6,7 +6,7 @@ The network (bd_surrogate_*, hand-written tcgen05 BF16 GEMMs) maps a setting
 to 34 outputs: F_s(k; t_w, t_w + t) of the big particles, log10 MSD of the
 big particles over the same window, and 32 samples of the total g(r) at time
 t_w + t.  The reference has no learned component; the engine is both the
-source of the training data and the judge of every proposal: a proposed
+source of the training data and the arbiter of every proposal: a proposed
 setting is always simulated before it is used.
 
 Proposal task.  For a fixed (phi, t_w, t, k), find the quench temperature
@@ -181,7 +181,7 @@ def propose_temperature(model, phi, log_tw, log_t, k, target=0.5, t_range=(0.05,
 
 
 def fs_at(settings, tw, lag, k, seeds, n_per_replica=1000, dt=1e-4):
-    """Plain simulation (the judge): F_s(k; t_w, t_w + lag) per setting,
+    """Plain simulation (the arbiter): F_s(k; t_w, t_w + lag) per setting,
     averaged over seeds, plus the sample rows of the whole run (8 lags up to
     `lag`, three wave numbers around k) for training."""
     reps = [s for s in settings for _ in seeds]
