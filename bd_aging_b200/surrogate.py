@@ -218,7 +218,7 @@ def crossing_study(phi=0.52, tw=100, lag=3000, k=7.0, budget=6, seeds=(1, 2, 3, 
     coarse grid, then proposals at the network's crossing and around it
     (each simulated, added to the training set, the network refitted), the
     estimate a least-squares line through the simulated points near the
-    proposals.  The truth is a dense plain sweep.  The simulations judge:
+    proposals.  The truth is a dense plain sweep.  The simulations decide:
     both estimates use simulated values only."""
     log_tw, log_t = math.log10(max(tw, 1) * dt), math.log10(lag * dt)
     ts_truth = np.linspace(t_range[0], t_range[1], truth_points)
