@@ -105,11 +105,16 @@ __device__ __forceinline__ unsigned long long mix64(unsigned long long x) {
 }
 
 // minibatch rows: x (FP32 [n_data][n_in]) -> X0 [B][k0] and X0^T [k0][B]
-// (BF16, zero padded), targets -> T [n_out_pad][B]
+// (BF16, zero padded), targets -> T [n_out_pad][B].  A block takes 32 rows
+// (lane = row), its warps split the columns: the transposed writes of a warp
+// are 32 consecutive rows.
+constexpr int kGatherRows = 32;
 __global__ void k_gather(const float *x, const float *y, int n_data, int n_in, int n_out, int k0, int n_out_pad,
                          int B, const int *rows, const long long *step, unsigned long long seed, __nv_bfloat16 *X0,
                          __nv_bfloat16 *X0t, float *T) {
-    const int r = blockIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int r = blockIdx.x * kGatherRows + lane;
+    if (r >= B) return;
     int src;
     if (rows) {
         src = rows[r];
@@ -118,14 +123,14 @@ __global__ void k_gather(const float *x, const float *y, int n_data, int n_in, i
                     (unsigned long long)n_data);
     }
     const bool valid = src >= 0 && src < n_data;
-    for (int k = threadIdx.x; k < k0; k += blockDim.x) {
+    for (int k = warp; k < k0; k += nw) {
         const float v = (valid && k < n_in) ? x[(size_t)src * n_in + k] : 0.f;
         const __nv_bfloat16 b = __float2bfloat16_rn(v);
         X0[(size_t)r * k0 + k] = b;
         X0t[(size_t)k * B + r] = b;
     }
     if (T)  // targets transposed [n_out_pad][B], as the loss epilogue reads them
-        for (int k = threadIdx.x; k < n_out_pad; k += blockDim.x)
+        for (int k = warp; k < n_out_pad; k += nw)
             T[(size_t)k * B + r] = (valid && k < n_out) ? y[(size_t)src * n_out + k] : 0.f;
 }
 
@@ -443,9 +448,9 @@ int adam(bd_surrogate *s) {
 }
 
 int train_step_launches(bd_surrogate *s) {
-    k_gather<<<s->batch, 64, 0, s->stream>>>(s->data_x, s->data_y, s->n_data, s->n_in, s->n_out, s->Kp[0],
-                                             s->Np[s->L - 1], s->batch, nullptr, s->step, s->seed, s->x0, s->ht[0],
-                                             s->t);
+    k_gather<<<div_up(s->batch, kGatherRows), 256, 0, s->stream>>>(
+        s->data_x, s->data_y, s->n_data, s->n_in, s->n_out, s->Kp[0], s->Np[s->L - 1], s->batch, nullptr, s->step,
+        s->seed, s->x0, s->ht[0], s->t);
     BD_LAUNCH_CHECK();
     int rc = forward(s, true);
     if (!rc) rc = backward(s);
@@ -687,8 +692,9 @@ int bd_surrogate_gradients(bd_surrogate *s, const float *x, const float *y, floa
     int *drows = nullptr;
     BD_CUDA_TRY(cudaMalloc(&drows, B * 4));
     cudaMemcpyAsync(drows, rows.data(), B * 4, cudaMemcpyHostToDevice, s->stream);
-    k_gather<<<B, 64, 0, s->stream>>>(dx, dy, B, s->n_in, s->n_out, s->Kp[0], s->Np[s->L - 1], B, drows, s->step,
-                                      s->seed, s->x0, s->ht[0], s->t);
+    k_gather<<<div_up(B, kGatherRows), 256, 0, s->stream>>>(dx, dy, B, s->n_in, s->n_out, s->Kp[0],
+                                                             s->Np[s->L - 1], B, drows, s->step, s->seed, s->x0,
+                                                             s->ht[0], s->t);
     int rc = forward(s, true);
     if (!rc) rc = backward(s);
     const int splits = B / s->ksplit;
@@ -740,8 +746,9 @@ int bd_surrogate_predict(bd_surrogate *s, const float *x, int n, float *y) {
         const int cnt = std::min(B, n - r0);
         for (int i = 0; i < B; i++) rows[i] = i < cnt ? r0 + i : -1;
         cudaMemcpyAsync(drows, rows.data(), B * 4, cudaMemcpyHostToDevice, s->stream);
-        k_gather<<<B, 64, 0, s->stream>>>(dx, nullptr, n, s->n_in, s->n_out, s->Kp[0], s->Np[s->L - 1], B, drows,
-                                          s->step, s->seed, s->x0, s->ht[0], nullptr);
+        k_gather<<<div_up(B, kGatherRows), 256, 0, s->stream>>>(dx, nullptr, n, s->n_in, s->n_out, s->Kp[0],
+                                                                 s->Np[s->L - 1], B, drows, s->step, s->seed,
+                                                                 s->x0, s->ht[0], nullptr);
         rc = forward(s, false);
         if (rc) break;
         cudaMemcpyAsync(hy.data(), s->y, hy.size() * 4, cudaMemcpyDeviceToHost, s->stream);
