@@ -23,13 +23,12 @@
 // CTA's MMA, which needed the peer's slice of the current operand, which the
 // peer sent after its own MMA of the previous GEMM had read the buffer.
 // Other shapes use per-thread distributed shared-memory stores and one
-// cluster barrier per GEMM.  The
-// weight-gradient GEMMs reduce over the batch and stay separate launches.
-// The next GEMM's weights are loaded while the epilogue of the current one
-// runs.  Every mbarrier wait is bounded: on expiry the CTA records an error
-// flag, waits (bounded) for its own copies, frees its tensor memory and
-// leaves the GEMM loop; the CTAs of a cluster agree on that at the cluster
-// barrier, so all of them pass the same barriers.
+// cluster barrier per GEMM.  The weight-gradient GEMMs reduce over the batch
+// and stay separate launches.  The next GEMM's weights are loaded while the
+// epilogue of the current one runs.  Every mbarrier wait is bounded: on
+// expiry the CTA records an error flag and skips its remaining MMAs and
+// epilogues while still passing every barrier of the cluster, then waits
+// (bounded) for its own copies and frees its tensor memory.
 #pragma once
 #include "umma.cuh"
 
