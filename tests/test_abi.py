@@ -81,3 +81,18 @@ def test_engine_rejects_bad_geometry_without_gpu():
                  dt=1e-5)
     with pytest.raises((B.BDError, RuntimeError)):
         B.Engine([s])
+
+
+def test_list_variant_count_matches_implementation():
+    """The public count of list-step launch variants (include/bd_aging.h) is
+    the engine's (csrc/nlist.cuh), so the ABI accepts exactly the variants the
+    engine launches."""
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    with open(os.path.join(root, "include", "bd_aging.h")) as f:
+        public = int(re.search(r"#define BD_LIST_VARIANTS (\d+)", f.read()).group(1))
+    with open(os.path.join(root, "bd_aging_b200", "csrc", "nlist.cuh")) as f:
+        src = f.read()
+    engine = int(re.search(r"constexpr int kListVariants = (\d+);", src).group(1))
+    assert public == engine
+    for v in range(engine):  # every variant has its launch parameters
+        assert re.search(r"struct ListVariant<%d> \{" % v, src), v
